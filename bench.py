@@ -1,0 +1,392 @@
+#!/usr/bin/env python3
+"""Headline benchmark: Gaussians/s (and ms/frame) of the point-splatting frame path at
+1080p, 4 spp, on the synthetic 16M-Gaussian town (supersampling 2, K = 4 points per thread,
+BVH-block + Hi-Z occlusion culling, TAA), stepping a 120-frame orbit one keyframe per frame.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl mine|reference] [--workload town16m|cube1m]
+
+One step = one frame (render + TAA post-process) through the library's C-ABI frame loop.
+`value` is whole-job Gaussians/s = N_scene x frames / device time (max over ranks); `e2e`
+repeats the timed loop through the same public call with the per-frame camera handed over
+from host memory and the u8 frame read back into pinned host memory every step.
+
+--gpus N > 1 (under torchrun): N independent replicas (the reference renders one view on one
+GPU; the path has no cross-GPU exchange), each rank on its own orbit phase; weak scaling.
+--impl reference: the reference has no CPU implementation of the path, so the CPU restatement
+of its algorithm (oracle/) is timed on the host cores on a bounded sample of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "gaussian-point-splatting_b200"))
+
+import synth  # noqa: E402
+
+SCENE_CACHE = os.path.join("/tmp", "gps_b200_scenes")
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+def workload_spec(name: str):
+    if name == "town16m":
+        return dict(n=16_000_000, kind="town", width=1920, height=1080, ss=2, spp=4, reduce=1, hier=1, occl=1,
+                    taa=1, frames=120)
+    if name == "cube1m":
+        return dict(n=1_000_000, kind="cube", width=640, height=360, ss=1, spp=1, reduce=1, hier=0, occl=0, taa=0,
+                    frames=1)
+    raise SystemExit(f"unknown workload {name}")
+
+
+def load_scene_host(spec) -> np.ndarray:
+    """Activated CPUGaussian array (N x 59 float32), cached on local disk per box."""
+    os.makedirs(SCENE_CACHE, exist_ok=True)
+    path = os.path.join(SCENE_CACHE, f"{spec['kind']}{spec['n']}_act.npy")
+    if os.path.exists(path):
+        return np.load(path, mmap_mode="r")
+    t = time.time()
+    raw = synth.town(spec["n"]) if spec["kind"] == "town" else synth.cube(spec["n"])
+    g = synth.activate(raw)
+    del raw
+    log(f"generated {spec['kind']} scene with {spec['n']} Gaussians in {time.time() - t:.1f}s")
+    tmp = path + f".{os.getpid()}.tmp.npy"
+    np.save(tmp, g)
+    os.replace(tmp, path)
+    return g
+
+
+def poses_for(spec):
+    if spec["kind"] == "town":
+        return synth.orbit(spec["frames"], 30.0, 10.0)
+    p = np.array([0.0, 0.0, -30.0])
+    return [(p, synth.look_at_c2w(p, [0.0, 0.0, 0.0]))]
+
+
+def settings_for(gpsplat, spec):
+    return gpsplat.default_settings(
+        width=spec["width"], height=spec["height"], supersampling_factor=spec["ss"], samples_per_pixel=spec["spp"],
+        reduce_point_count=spec["reduce"], enable_hierarchical_culling=spec["hier"],
+        fully_disable_hierarchical_culling=0 if spec["hier"] else 1, enable_occlusion_culling=spec["occl"],
+        accumulation_mode=gpsplat.GPS_ACCUM_TAA if spec["taa"] else gpsplat.GPS_ACCUM_NONE)
+
+
+def make_cameras(gpsplat, settings, poses, count, phase):
+    cams = []
+    for i in range(count):
+        p, r = poses[(phase + i) % len(poses)]
+        c = gpsplat.camera_from_pose(p, np.asarray(r, np.float32).T, settings, i + 1)
+        c.camera_moved = 1
+        cams.append(c)
+    return cams
+
+
+class ClockSampler:
+    """nvidia-smi samples during the timed region (SM clock, max clock, throttle reasons)."""
+
+    FIELDS = "clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap"
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 7:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                mx.append(float(parts[1]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[3:7]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_init():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    return world, rank, local
+
+
+def max_over_ranks(x: float, world: int) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world: int):
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+# ---------------------------------------------------------------------------------
+# CPU baseline (the oracle, oracle/oracle.cpp) on a bounded sample of the workload
+# ---------------------------------------------------------------------------------
+def cpu_baseline(gpsplat, g_host, spec, settings, poses, budget_s: float = 12.0):
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+
+    cores = os.cpu_count() or 1
+    n_total = g_host.shape[0]
+    sample_n = min(n_total, 1_000_000)
+    sub = np.ascontiguousarray(g_host[:sample_n])
+    o = oracle.Oracle(sub, settings, threads=cores)
+    cams = make_cameras(gpsplat, settings, poses, max(1, len(poses)), 0)
+    t0 = time.time()
+    frames = 0
+    while True:
+        o.render(cams[frames % len(cams)])
+        frames += 1
+        if time.time() - t0 > budget_s or frames >= 64:
+            break
+    dt = time.time() - t0
+    o.close()
+    return {"value": sample_n * frames / dt, "unit": "Gaussians/s", "cores": cores, "kind": "port",
+            "sample": f"first {sample_n} of {n_total} Gaussians (Morton-ordered contiguous block), {frames} frames "
+                      f"of the same camera path and settings, {dt:.1f}s"}
+
+
+def run_reference_arm(args, spec, world, rank):
+    if rank != 0:
+        return 0
+    import gpsplat
+
+    gpsplat.load_library()
+    g = load_scene_host(spec)
+    s = settings_for(gpsplat, spec)
+    poses = poses_for(spec)
+    per_step = []
+    cb = None
+    for k in range(args.warmup + args.steps):
+        cb = cpu_baseline(gpsplat, g, spec, s, poses, budget_s=max(2.0, 20.0 / max(1, args.steps)))
+        if k >= args.warmup:
+            per_step.append(cb["value"])
+    value = float(np.mean(per_step))
+    cb["value"] = value
+    line = {"impl": "reference", "metric": "Gaussians/sec", "value": value, "unit": "Gaussians/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded town, see synth.py)",
+            "config": {"workload": args.workload, "gaussians": spec["n"], "resolution": [spec["width"], spec["height"]],
+                       "supersampling": spec["ss"], "spp": spec["spp"], "culling": bool(spec["hier"]),
+                       "taa": bool(spec["taa"])},
+            "cpu_baseline": cb,
+            "e2e": {"value": value, "unit": "Gaussians/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ---------------------------------------------------------------------------------
+# the GPU arm
+# ---------------------------------------------------------------------------------
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=30)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="mine", choices=["mine", "reference"])
+    ap.add_argument("--workload", default="town16m", choices=["town16m", "cube1m"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(3, args.warmup)
+    spec = workload_spec(args.workload)
+    world, rank, local = dist_init()
+    if args.impl == "reference":
+        return run_reference_arm(args, spec, world, rank)
+
+    import torch
+
+    torch.cuda.set_device(local)
+    import gpsplat
+
+    gpsplat.load_library()
+    g_host = load_scene_host(spec)
+    t = time.time()
+    scene = gpsplat.Scene.from_host(np.ascontiguousarray(g_host), presorted=True)
+    log(f"rank {rank}: scene uploaded in {time.time() - t:.1f}s")
+    s = settings_for(gpsplat, spec)
+    r = gpsplat.Renderer(scene, s)
+    loop = gpsplat.FrameLoop(r)
+    poses = poses_for(spec)
+    phase = (rank * len(poses)) // max(1, world)
+    total = args.warmup + args.steps
+    cams = make_cameras(gpsplat, s, poses, total, phase)
+    stream = torch.cuda.Stream()
+    sh = stream.cuda_stream
+
+    # warm-up
+    for c in cams[: args.warmup]:
+        loop.step(c, sh)
+    torch.cuda.synchronize()
+    r.enable_timing(False)
+
+    # ---- device-timed region: K frames, inputs resident (scene > L2 every frame) ----
+    sampler = ClockSampler(local)
+    barrier(world)
+    torch.cuda.synchronize()
+    sampler.start()
+    time.sleep(0.3)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for c in cams[args.warmup:]:
+        loop.step(c, sh)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier(world)
+    clocks = sampler.stop()
+    dev_ms = e0.elapsed_time(e1)
+    dev_ms_max = max_over_ranks(dev_ms, world)
+    st = r.stats()
+    launches_per_frame = st.kernel_launches
+
+    # ---- per-stage times (separate timed pass with CUDA events between stages) ----
+    r.enable_timing(True)
+    r.stage_times(reset=True)
+    for c in cams[args.warmup:]:
+        loop.step(c, sh)
+    torch.cuda.synchronize()
+    stages = r.stage_times(reset=True)
+    r.enable_timing(False)
+
+    # ---- end to end through the public call with host buffers ----
+    h, w = s.height, s.width
+    host_frame = torch.empty((h, w, 3), dtype=torch.uint8, pin_memory=True)
+    cam_bytes = len(bytes(cams[0]))
+    barrier(world)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    e2 = torch.cuda.Event(enable_timing=True)
+    e3 = torch.cuda.Event(enable_timing=True)
+    e2.record(stream)
+    for c in cams[args.warmup:]:
+        loop.step(c, sh)  # camera handed over from host memory
+        loop.read(host_frame.numpy(), sh)  # u8 frame back to pinned host memory (synchronises)
+    e3.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = max_over_ranks(e2.elapsed_time(e3), world)
+    wall_e2e = time.perf_counter() - t0
+    barrier(world)
+
+    n_scene = scene.count
+    K = args.steps
+    value = n_scene * K * world / (dev_ms_max / 1000.0)
+    e2e_value = n_scene * K * world / (e2e_ms / 1000.0)
+
+    # roofline of the dominant kernel
+    peaks = {}
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            peaks = json.load(f)
+    except OSError:
+        pass
+    hbm_peak = float(peaks.get("hbm_gbs", 6650.0))
+    peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
+    dom = max(stages, key=lambda k: stages[k][0])
+    dom_ms, dom_launches = stages[dom]
+    per_launch_ms = dom_ms / max(1, dom_launches)
+    ntot = n_scene
+    entries = r.splat_buffer()[1]
+    surv = st.survivors_one + st.survivors_two
+    passes = 2 if spec["occl"] else 1
+    if dom == "splat":
+        # compulsory traffic of a splat launch: each survivor's 64-byte record and 8 bytes of
+        # workload, one read and one write of every splat-buffer entry
+        alg_bytes = (72.0 * surv / passes) + 16.0 * entries
+    elif dom == "preprocess":
+        alg_bytes = ntot * 48.0 + (surv / passes) * (192.0 + 64.0 + 4.0) + ntot / 8.0
+    elif dom == "resolve":
+        alg_bytes = 8.0 * entries + 16.0 * w * h
+    else:
+        alg_bytes = 8.0 * entries
+    achieved = alg_bytes / (per_launch_ms / 1000.0) / 1e9
+    roofline = {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
+                "frac": achieved / hbm_peak, "traffic": None, "peak_source": peak_src,
+                "algorithmic_bytes_per_launch": alg_bytes, "ms_per_launch": per_launch_ms}
+
+    line = {
+        "metric": "Gaussians/sec", "value": value, "unit": "Gaussians/s", "n_gpus": world, "steps": K,
+        "warmup": args.warmup, "ms_per_step": dev_ms_max / K, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded town, see synth.py)",
+        "config": {"workload": args.workload, "gaussians": n_scene, "resolution": [w, h], "supersampling": spec["ss"],
+                   "spp": spec["spp"], "points_per_thread": spec["ss"] ** 2 if spec["reduce"] else 1,
+                   "culling": bool(spec["hier"]), "occlusion": bool(spec["occl"]), "taa": bool(spec["taa"]),
+                   "camera_path": f"{len(poses)}-frame orbit r=30 h=10" if spec["kind"] == "town" else "static",
+                   "l2": "inputs larger than L2 (scene >= 3.8 GB read every frame)", "parallelism": f"replicas x{world}"},
+        "clocks": clocks,
+        "e2e": {"value": e2e_value, "unit": "Gaussians/s", "h2d_bytes_per_step": cam_bytes,
+                "d2h_bytes_per_step": h * w * 3, "ms_per_step": e2e_ms / K, "wall_s": wall_e2e},
+        "gpu_launches": int(launches_per_frame * K),
+        "roofline": roofline,
+        "stages_ms_per_frame": {k: v[0] / K for k, v in stages.items()},
+        "points_per_frame": [st.num_points_one, st.num_points_two],
+        "survivors_per_frame": [st.survivors_one, st.survivors_two],
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(gpsplat, g_host, spec, s, poses)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    loop.close()
+    r.close()
+    scene.close()
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

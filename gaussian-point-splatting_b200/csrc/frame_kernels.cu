@@ -1,0 +1,809 @@
+// sm_100a kernels of the Gaussian point-splatting frame path.
+//
+//   block cull    gaussian_bvh.cu:215-329          one thread per block node, warp ballot
+//   preprocess    gaussian_point_splatting.cu:17-65,147-307
+//   scan          workload_distributor.cu:52-145   single-pass decoupled look-back scan that
+//                                                  compacts survivors and keeps P on the device
+//   splat         gaussian_point_splatting.cu:67-141,383-432  persistent, tile-of-points blocks
+//   clear/resolve gaussian_point_splatting.cu:484-548,580-585
+//   Hi-Z          depth_mip_chain.cu:7-145, depth_mip_chain.cuh:172-215
+//   TAA/progress  post_processing_kernels.cuh:108-285
+//
+// Every floating-point expression that decides a sample position, a count or a packed
+// value follows the reference's expression shape (see gps_math.cuh) so that the 64-bit
+// splat buffer is bit-identical to the reference kernels' for the same inputs.
+#include <cstdio>
+#include "frame_kernels.h"
+#include "gps_rng.cuh"
+
+namespace gps {
+
+namespace {
+
+constexpr int kScanThreads = 256;
+constexpr int kScanItems = 16;
+constexpr uint32_t kScanTile = kScanThreads * kScanItems;  // 4096 Gaussians per scan tile
+constexpr int kSpinLimit = 1 << 22;                         // bounded look-back wait
+
+// ---------------------------------------------------------------------------------
+// Hi-Z query (depth_mip_chain.cuh:172-215, the non-tree variant the reference compiles)
+// ---------------------------------------------------------------------------------
+__device__ __forceinline__ bool hiz_occluded(const HizView& c, float depth, ivec2 mn, ivec2 mx) {
+    mn.x = max(0, mn.x);
+    mn.y = max(0, mn.y);
+    mx.x = min(c.width - 1, mx.x);
+    mx.y = min(c.height - 1, mx.y);
+    int w = mx.x - mn.x + 1;
+    int h = mx.y - mn.y + 1;
+    int d = max(w, h);
+    int lod = (int)ceilf(log2f((float)d / 2.0f));
+    lod = min(max(lod, 0), c.levels - 1);
+    int l = (c.levels - 1) - lod;
+    const int wl = c.level_w[l];
+    const int hl = c.level_h[l];
+    int tile_w = max(1, min(c.width, 1 << (c.levels - l - 1)));
+    int tile_h = max(1, min(c.height, 1 << (c.levels - l - 1)));
+    int tx0 = max(0, min(wl - 1, mn.x / tile_w));
+    int ty0 = max(0, min(hl - 1, mn.y / tile_h)) * wl;
+    int tx1 = max(0, min(wl - 1, mx.x / tile_w));
+    int ty1 = max(0, min(hl - 1, mx.y / tile_h)) * wl;
+    const float* base = c.mip + c.level_off[l];
+    float zmax = fmaxf(base[tx0 + ty0], fmaxf(base[tx1 + ty0], fmaxf(base[tx0 + ty1], base[tx1 + ty1])));
+    return zmax < depth;
+}
+
+__device__ __forceinline__ bool block_culled(const BlockView& b, uint32_t g) {
+    uint32_t node = g / b.per_block;
+    return ((__ldg(&b.culled[node >> 5]) >> (node & 31)) & 1u) != 0u;
+}
+
+__device__ __forceinline__ bool mask_bit(const uint32_t* m, uint32_t g) {
+    return ((__ldg(&m[g >> 5]) >> (g & 31)) & 1u) != 0u;
+}
+
+// ---------------------------------------------------------------------------------
+// Block cull (gaussian_bvh.cu:215-329)
+// ---------------------------------------------------------------------------------
+__device__ __forceinline__ bool aabb_outside_frustum(vec3 bmin, vec3 bmax, const vec4* planes) {
+#pragma unroll
+    for (int i = 0; i < 6; ++i) {
+        const vec3 n = make_v3(planes[i].x, planes[i].y, planes[i].z);
+        const float d = planes[i].w;
+        vec3 v = make_v3(n.x >= 0.0f ? bmax.x : bmin.x, n.y >= 0.0f ? bmax.y : bmin.y, n.z >= 0.0f ? bmax.z : bmin.z);
+        if (dot(n, v) + d < 0.0f) return true;
+    }
+    return false;
+}
+
+__device__ __forceinline__ bool aabb_project_bounds(vec3 bmin, vec3 bmax, const mat4& vp, int width, int height,
+                                                    ivec2& out_min, ivec2& out_max, float& out_depth) {
+    vec3 corners[8] = {{bmin.x, bmin.y, bmin.z}, {bmax.x, bmin.y, bmin.z}, {bmin.x, bmax.y, bmin.z},
+                       {bmax.x, bmax.y, bmin.z}, {bmin.x, bmin.y, bmax.z}, {bmax.x, bmin.y, bmax.z},
+                       {bmin.x, bmax.y, bmax.z}, {bmax.x, bmax.y, bmax.z}};
+    int minx = width - 1, miny = height - 1, maxx = 0, maxy = 0;
+    float min_depth = 1e30f;
+    bool any_front = false;
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+        vec4 clip = vp * make_v4(corners[i].x, corners[i].y, corners[i].z, 1.0f);
+        if (clip.w <= 0.0f) continue;
+        any_front = true;
+        vec3 ndc = make_v3(clip.x / clip.w, clip.y / clip.w, clip.z / clip.w);
+        int px = int((ndc.x * 0.5f + 0.5f) * width);
+        int py = int((ndc.y * 0.5f + 0.5f) * height);
+        minx = min(minx, px);
+        miny = min(miny, py);
+        maxx = max(maxx, px);
+        maxy = max(maxy, py);
+        min_depth = fminf(min_depth, ndc.z);
+    }
+    if (!any_front) return false;
+    minx = max(minx, 0);
+    miny = max(miny, 0);
+    maxx = min(maxx, width - 1);
+    maxy = min(maxy, height - 1);
+    if (minx > maxx || miny > maxy) return false;
+    out_min = {minx, miny};
+    out_max = {maxx, maxy};
+    out_depth = min_depth;
+    return true;
+}
+
+__global__ void __launch_bounds__(256) block_cull_kernel(BlockView b, FrameConst fc, HizView hiz) {
+    const uint32_t idx = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t word = (idx & ~31u) >> 5;
+    if (word >= b.words) return;
+    bool culled = false;
+    if (idx < b.node_count) {
+        float4 lo = __ldg(&b.nodes[2 * idx]);
+        float4 hi = __ldg(&b.nodes[2 * idx + 1]);
+        vec3 bmin = make_v3(lo.x, lo.y, lo.z), bmax = make_v3(hi.x, hi.y, hi.z);
+        if (aabb_outside_frustum(bmin, bmax, fc.planes)) {
+            culled = true;
+        } else if (fc.enable_occlusion) {
+            ivec2 mn, mx;
+            float front;
+            if (aabb_project_bounds(bmin, bmax, fc.vp, hiz.width, hiz.height, mn, mx, front))
+                culled = hiz_occluded(hiz, front, mn, mx);
+        }
+    }
+    __syncwarp();
+    unsigned m = __ballot_sync(0xffffffffu, culled);
+    if ((threadIdx.x & 31) == 0) b.culled[word] = m;
+}
+
+// ---------------------------------------------------------------------------------
+// Preprocess (gaussian_point_splatting.cu:17-65 + 147-307)
+// ---------------------------------------------------------------------------------
+template <class Scene>
+__global__ void __launch_bounds__(256) preprocess_kernel(PreprocessArgs a, Scene scene) {
+    const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+    const FrameConst& fc = a.fc;
+    u32x2 seed = make_seed((uint32_t)idx, (uint32_t)a.frame_seed);
+    bool splats = false;
+    do {
+        if (idx >= (int)a.n) break;
+        if (fc.enable_hier && block_culled(a.blocks, (uint32_t)idx)) break;
+        if (a.only_previously_occluded && mask_bit(a.mask_prev, (uint32_t)idx)) break;
+        float opacity = scene.opacity((uint32_t)idx);
+        if (opacity <= 0.0f) break;
+
+        vec3 mean, scale;
+        vec4 quat;
+        scene.geometry((uint32_t)idx, mean, quat, scale);
+        // loadAndTransformGaussian
+        vec3 view_mean = transform_point4x3(mean, fc.view);
+        float view_z = view_mean.z;
+        if (-view_z <= 0.2f) break;
+        vec4 proj_mean = fc.vp * make_v4(mean.x, mean.y, mean.z, 1.0f);
+        proj_mean = proj_mean * (1.0f / proj_mean.w);
+        if (proj_mean.z < -1.0f || proj_mean.z > 1.0f) break;
+        mat3 cov = scale_rot_to_cov(scale, quat);
+        vec3 cov2d = compute_cov2d(fc.view, cov, mean, fc.tan_fov, fc.focal);
+        const float dil = 0.3f * (float)fc.ss * (float)fc.ss;
+        cov2d = cov2d + make_v3(dil, 0.0f, dil);
+        float det = cov2d.x * cov2d.z - cov2d.y * cov2d.y;
+        if (det <= 0.0f) break;
+        vec2 pixel_mean = make_v2((proj_mean.x * 0.5f + 0.5f) * (float)fc.up_width,
+                                  (proj_mean.y * 0.5f + 0.5f) * (float)fc.up_height);
+        ivec2 pmin, pmax;
+        if (!gaussian_tile_bounds(pmin, pmax, {fc.up_width, fc.up_height}, cov2d, pixel_mean)) break;
+
+        if (pmin.x >= fc.up_width || pmin.y >= fc.up_height || pmax.x < 0 || pmax.y < 0) break;
+        if (fc.cull_small) {
+            float trace = cov2d.x + cov2d.z;
+            float half = 0.5f * trace;
+            float term2 = __fsqrt_rn(fmaxf(0.1f, half * half - det));
+            float e1 = half + term2;
+            float e2 = half - term2;
+            if (e1 < 0.02f || e2 < 0.02f) break;
+        }
+        constexpr float kTwoPi = 2.0f * 3.14159265358979323846f;
+        float importance;
+        float s_det = __fsqrt_rn(det);
+        if (fc.use_unbiased) importance = kTwoPi * s_det * dilog(opacity);
+        else importance = opacity * kTwoPi * s_det;
+
+        if (fc.enable_occlusion) {
+            ivec2 qmin = {pmin.x / fc.ss, pmin.y / fc.ss};
+            ivec2 qmax = {pmax.x / fc.ss, pmax.y / fc.ss};
+            if (hiz_occluded(a.hiz, proj_mean.z, qmin, qmax)) break;
+        }
+        float kf = (float)(fc.ss * fc.ss * kPointsPerKernel);
+        if (!fc.reduce_point_count) kf = 1.0f;
+        uint32_t num_points;
+        if (fc.use_unbiased) num_points = poisson(seed, importance);
+        else num_points = (uint32_t)stochastic_round(importance, pcg2d(seed).x);
+        if (kf > 1) num_points = (uint32_t)stochastic_round((float)num_points / kf, pcg2d(seed).x);
+        if (num_points <= 0) break;
+        uint32_t cap = (uint32_t)(fc.up_width * fc.up_height / (2 * kf));
+        num_points = (cap < num_points) ? cap : num_points;
+
+        vec3 campos = make_v3(fc.cam.c[3].x, fc.cam.c[3].y, fc.cam.c[3].z);
+        vec3 color = scene.color((uint32_t)idx, mean, campos);
+
+        // per-Gaussian prologue of splatGaussianPoint (gaussian_point_splatting.cu:88-96)
+        const uint64_t view_depth_bits = depth_key(view_z, fc.near_plane, fc.far_plane) << kDepthShift;
+        vec3 conic = conic_of(cov2d, 1.0f / det);
+        const float c0 = __fsqrt_rn(cov2d.x);
+        const float c1 = cov2d.y / c0;
+        const float c2 = __fsqrt_rn(cov2d.z - c1 * c1);
+        uint32_t r12 = (uint32_t)(color.x * 255.0f) & 0xFFFu;
+        uint32_t g12 = (uint32_t)(color.y * 255.0f) & 0xFFFu;
+        uint32_t b12 = (uint32_t)(color.z * 255.0f) & 0xFFFu;
+        uint64_t key = view_depth_bits | (uint64_t(r12) << 24) | (uint64_t(g12) << 12) | uint64_t(b12);
+
+        SplatRecord rec;
+        rec.a = make_float4(pixel_mean.x, pixel_mean.y, c0, c1);
+        rec.b = make_float4(c2, conic.x, conic.y, conic.z);
+        rec.c = make_float4(opacity, color.x, color.y, color.z);
+        rec.d = make_uint4((uint32_t)pmin.x | ((uint32_t)pmin.y << 16), (uint32_t)pmax.x | ((uint32_t)pmax.y << 16),
+                           (uint32_t)key, (uint32_t)(key >> 32));
+        a.records[idx] = rec;
+        a.counts[idx] = num_points;
+        splats = true;
+    } while (false);
+
+    const unsigned m = __ballot_sync(0xffffffffu, splats);
+    if ((threadIdx.x & 31) == 0) {
+        const uint32_t warp_base = (uint32_t)idx & ~31u;
+        if (warp_base < a.n) a.mask_cur[warp_base >> 5] = m;
+    }
+}
+
+// ---------------------------------------------------------------------------------
+// Scan: single-pass decoupled look-back over (survivor count, point count) pairs
+// (replaces workload_distributor.cu:62-145: 3 blocking D2H copies, an exclusive scan,
+// a scatter and a P-long max-scan).  Status word: [63:62] flag, [61:32] survivors,
+// [31:0] points (mod 2^32 like the reference's u32 offsets).
+// ---------------------------------------------------------------------------------
+constexpr unsigned long long kFlagAgg = 1ull << 62;
+constexpr unsigned long long kFlagInc = 2ull << 62;
+
+__device__ __forceinline__ unsigned long long pack_status(unsigned long long flag, uint32_t surv, uint32_t pts) {
+    return flag | ((unsigned long long)(surv & 0x3FFFFFFFu) << 32) | pts;
+}
+
+__global__ void __launch_bounds__(kScanThreads) scan_kernel(ScanArgs a) {
+    __shared__ uint32_t s_tile;
+    __shared__ uint32_t s_warp_surv[kScanThreads / 32];
+    __shared__ uint32_t s_warp_pts[kScanThreads / 32];
+    __shared__ uint32_t s_prefix_surv, s_prefix_pts;
+    if (threadIdx.x == 0) s_tile = atomicAdd(a.tile_ticket, 1u);
+    __syncthreads();
+    const uint32_t tile = s_tile;
+    const uint32_t num_tiles = (a.n + kScanTile - 1) / kScanTile;
+    const uint32_t base = tile * kScanTile + threadIdx.x * kScanItems;
+
+    uint32_t bits = 0;
+    uint32_t cnt[kScanItems];
+    if (base < a.n) {
+        bits = (__ldg(&a.mask[base >> 5]) >> (base & 31)) & 0xFFFFu;
+        if (a.n - base < (uint32_t)kScanItems) bits &= (1u << (a.n - base)) - 1u;
+    }
+#pragma unroll
+    for (int q = 0; q < kScanItems / 4; ++q) {
+        uint4 v = make_uint4(0, 0, 0, 0);
+        if ((bits >> (4 * q)) & 0xFu) v = __ldg(reinterpret_cast<const uint4*>(a.counts + base) + q);
+        cnt[4 * q + 0] = ((bits >> (4 * q + 0)) & 1u) ? v.x : 0u;
+        cnt[4 * q + 1] = ((bits >> (4 * q + 1)) & 1u) ? v.y : 0u;
+        cnt[4 * q + 2] = ((bits >> (4 * q + 2)) & 1u) ? v.z : 0u;
+        cnt[4 * q + 3] = ((bits >> (4 * q + 3)) & 1u) ? v.w : 0u;
+    }
+    uint32_t t_surv = __popc(bits);
+    uint32_t t_pts = 0;
+#pragma unroll
+    for (int i = 0; i < kScanItems; ++i) t_pts += cnt[i];
+
+    // block-wide inclusive scan of the per-thread aggregates
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    uint32_t inc_surv = t_surv, inc_pts = t_pts;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        uint32_t vs = __shfl_up_sync(0xffffffffu, inc_surv, o);
+        uint32_t vp = __shfl_up_sync(0xffffffffu, inc_pts, o);
+        if (lane >= o) {
+            inc_surv += vs;
+            inc_pts += vp;
+        }
+    }
+    if (lane == 31) {
+        s_warp_surv[warp] = inc_surv;
+        s_warp_pts[warp] = inc_pts;
+    }
+    __syncthreads();
+    uint32_t warp_off_surv = 0, warp_off_pts = 0, blk_surv = 0, blk_pts = 0;
+#pragma unroll
+    for (int w = 0; w < kScanThreads / 32; ++w) {
+        if (w < warp) {
+            warp_off_surv += s_warp_surv[w];
+            warp_off_pts += s_warp_pts[w];
+        }
+        blk_surv += s_warp_surv[w];
+        blk_pts += s_warp_pts[w];
+    }
+    uint32_t ex_surv = warp_off_surv + inc_surv - t_surv;
+    uint32_t ex_pts = warp_off_pts + inc_pts - t_pts;
+
+    // decoupled look-back (warp 0)
+    volatile unsigned long long* state = a.tile_state;
+    if (warp == 0) {
+        uint32_t pre_surv = 0, pre_pts = 0;
+        if (tile == 0) {
+            if (lane == 0) state[0] = pack_status(kFlagInc, blk_surv, blk_pts);
+        } else {
+            if (lane == 0) state[tile] = pack_status(kFlagAgg, blk_surv, blk_pts);
+            int window_end = (int)tile - 1;  // look at tiles window_end - lane
+            bool done = false;
+            bool timeout = false;
+            while (!done) {
+                int t = window_end - lane;
+                unsigned long long s = 0;
+                if (t >= 0) {
+                    int spins = 0;
+                    s = state[t];
+                    while ((s >> 62) == 0ull) {
+                        if (++spins > kSpinLimit) {
+                            timeout = true;
+                            break;
+                        }
+                        __nanosleep(64);
+                        s = state[t];
+                    }
+                } else {
+                    s = kFlagInc;  // virtual inclusive zero before tile 0
+                }
+                if (__any_sync(0xffffffffu, timeout)) {
+                    if (lane == 0) atomicExch(&a.counters->scan_timeouts, 1u);
+                    break;
+                }
+                unsigned inc_mask = __ballot_sync(0xffffffffu, (s >> 62) == 2ull);
+                int first_inc = inc_mask ? __ffs(inc_mask) - 1 : 32;  // closest tile with inclusive prefix
+                uint32_t vs = (lane <= first_inc) ? (uint32_t)((s >> 32) & 0x3FFFFFFFu) : 0u;
+                uint32_t vp = (lane <= first_inc) ? (uint32_t)(s & 0xFFFFFFFFu) : 0u;
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) {
+                    vs += __shfl_xor_sync(0xffffffffu, vs, o);
+                    vp += __shfl_xor_sync(0xffffffffu, vp, o);
+                }
+                pre_surv += vs;
+                pre_pts += vp;
+                if (inc_mask) done = true;
+                else window_end -= 32;
+            }
+            if (lane == 0) state[tile] = pack_status(kFlagInc, pre_surv + blk_surv, pre_pts + blk_pts);
+        }
+        if (lane == 0) {
+            s_prefix_surv = pre_surv;
+            s_prefix_pts = pre_pts;
+            if (tile == num_tiles - 1) {
+                uint32_t total = pre_pts + blk_pts;
+                a.counters->survivors = pre_surv + blk_surv;
+                a.counters->total_points = total;
+                a.counters->points = total < a.max_points ? total : a.max_points;
+                a.counters->truncated = total > a.max_points ? 1u : 0u;
+            }
+        }
+    }
+    __syncthreads();
+    uint32_t r = s_prefix_surv + ex_surv;
+    uint32_t pt = s_prefix_pts + ex_pts;
+#pragma unroll
+    for (int i = 0; i < kScanItems; ++i) {
+        if ((bits >> i) & 1u) {
+            a.surv_gid[r] = base + i;
+            a.surv_start[r] = pt;
+            // first survivor of every splat tile that starts inside [pt, pt + cnt) below the budget
+            unsigned long long lo = pt, hi = (unsigned long long)pt + cnt[i];
+            if (hi > a.max_points) hi = a.max_points;
+            unsigned long long t0 = (lo + a.tile_points - 1) / a.tile_points;
+            for (unsigned long long t = t0; t * a.tile_points < hi; ++t) a.tile_first_rank[t] = r;
+            ++r;
+            pt += cnt[i];
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------------
+// Splat (gaussian_point_splatting.cu:67-141 with num_points = 1, 383-432)
+// ---------------------------------------------------------------------------------
+constexpr int kSplatTile = 256;
+
+__device__ __forceinline__ void atomic_add_color(unsigned long long* address, uint64_t value) {
+    // post_processing_kernels.cuh:13-42 with add_if_equal = true
+    const uint64_t target_depth = value & kDepthMask;
+    unsigned long long old = *address, assumed;
+    do {
+        assumed = old;
+        uint64_t assumed_depth = assumed & kDepthMask;
+        uint64_t new_value = value;
+        if (target_depth > assumed_depth) return;
+        if (target_depth == assumed_depth) {
+            uint64_t new_lower = (assumed & kColorMask) + (value & kColorMask);
+            new_value = (assumed & kDepthMask) | (new_lower & kColorMask);
+        }
+        old = atomicCAS(address, assumed, (unsigned long long)new_value);
+    } while (assumed != old);
+}
+
+__device__ __forceinline__ void splat_point(uint32_t point, const SplatRecord& rec, const FrameConst& fc,
+                                            int frame_seed, uint64_t* __restrict__ buffer) {
+    u32x2 seed = make_seed(point, (uint32_t)frame_seed);
+    const vec2 pixel_mean = make_v2(rec.a.x, rec.a.y);
+    const float c0 = rec.a.z, c1 = rec.a.w, c2 = rec.b.x;
+    const vec3 conic = make_v3(rec.b.y, rec.b.z, rec.b.w);
+    const float opacity = rec.c.x;
+    const int minx = (int)(rec.d.x & 0xFFFFu), miny = (int)(rec.d.x >> 16);
+    const int maxx = (int)(rec.d.y & 0xFFFFu), maxy = (int)(rec.d.y >> 16);
+    const uint64_t key = (uint64_t)rec.d.z | ((uint64_t)rec.d.w << 32);
+    const uint64_t view_depth_bits = key & kDepthMask;
+    int k = fc.ss * fc.ss * kPointsPerKernel;
+    if (!fc.reduce_point_count) k = 1;
+    const int samples = fc.num_passes * k;
+    for (int p = 0; p < samples; ++p) {
+        vec2 u = pcg2d(seed);
+        vec2 xy;
+        if (fc.use_unbiased) xy = corrected_box_muller(u.x, u.y, opacity);
+        else xy = box_muller(u.x, u.y);
+        vec2 pixel = make_v2(pixel_mean.x + c0 * xy.x, pixel_mean.y + c1 * xy.x + c2 * xy.y);
+        pixel = make_v2(floorf(pixel.x), floorf(pixel.y));
+        int x = (int)pixel.x;
+        int y = (int)pixel.y;
+        vec2 delta = make_v2(pixel_mean.x - pixel.x, pixel_mean.y - pixel.y);
+        if (x < minx || x >= maxx || y < miny || y >= maxy) continue;
+        float gw = gaussian_value(conic, delta);
+        float alpha = opacity * gw;
+        if (alpha < 1.0f / 255.0f) continue;
+        int index = splat_index(x, y, p / k, fc.num_passes, fc.up_width, fc.up_height);
+        unsigned long long* slot = reinterpret_cast<unsigned long long*>(buffer + index);
+        if ((uint64_t)__ldcg(slot) <= view_depth_bits) continue;
+        if (fc.use_unbiased) atomicMin(slot, (unsigned long long)key);
+        else atomic_add_color(slot, key);
+    }
+}
+
+__global__ void __launch_bounds__(kSplatTile) splat_kernel(SplatArgs a) {
+    __shared__ uint32_t s_start[kSplatTile];
+    const uint32_t points = a.counters->points;
+    const uint32_t survivors = a.counters->survivors;
+    for (uint32_t tile = blockIdx.x; (unsigned long long)tile * kSplatTile < points; tile += gridDim.x) {
+        const uint32_t p0 = tile * kSplatTile;
+        const uint32_t r0 = a.tile_first_rank[tile];
+        {
+            uint32_t r = r0 + threadIdx.x;
+            s_start[threadIdx.x] = (r0 < survivors && r < survivors) ? a.surv_start[r] : 0xFFFFFFFFu;
+        }
+        __syncthreads();
+        const uint32_t p = p0 + threadIdx.x;
+        if (p < points && s_start[0] <= p) {
+            int lo = 0, hi = kSplatTile - 1;  // largest k with s_start[k] <= p
+            while (lo < hi) {
+                int mid = (lo + hi + 1) >> 1;
+                if (s_start[mid] <= p) lo = mid;
+                else hi = mid - 1;
+            }
+            const uint32_t g = __ldg(&a.surv_gid[r0 + lo]);
+            if (g < a.n) {  // always true unless the scan gave up (device_timeouts)
+                const float4* rp = reinterpret_cast<const float4*>(a.records + g);
+                SplatRecord rec;
+                rec.a = __ldg(rp + 0);
+                rec.b = __ldg(rp + 1);
+                rec.c = __ldg(rp + 2);
+                rec.d = __ldg(reinterpret_cast<const uint4*>(rp + 3));
+                splat_point(p, rec, a.fc, a.frame_seed, a.buffer);
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------------------------
+// Clear and resolve (gaussian_point_splatting.cu:484-548, 580-585)
+// ---------------------------------------------------------------------------------
+__global__ void clear_kernel(ulonglong2* __restrict__ buf, uint64_t pairs, unsigned long long value) {
+    const ulonglong2 v = make_ulonglong2(value, value);
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < pairs; i += (uint64_t)gridDim.x * blockDim.x)
+        buf[i] = v;
+}
+
+template <bool kDepthOnly>
+__global__ void __launch_bounds__(256) resolve_kernel(ResolveArgs a) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y * blockDim.y + threadIdx.y;
+    if (x >= a.width || y >= a.height) return;
+    const uint32_t idx = (uint32_t)(y * a.width + x);
+    const int bx = x * a.ss, by = y * a.ss;
+    const int up_w = a.width * a.ss, up_h = a.height * a.ss;
+    float depth = 1e9f;
+    vec3 color = make_v3(0.0f, 0.0f, 0.0f);
+    for (int dx = 0; dx < a.ss; dx++)
+        for (int dy = 0; dy < a.ss; dy++)
+            for (int p = 0; p < a.num_passes; ++p) {
+                int i = splat_index(bx + dx, by + dy, p, a.num_passes, up_w, up_h);
+                if ((uint64_t)(int64_t)i >= a.entries) continue;
+                uint64_t val = __ldcs(reinterpret_cast<const unsigned long long*>(a.buffer) + i);
+                float view_depth = view_depth_from_key((val >> 36ull) & kDepthMax, a.near_plane, a.far_plane);
+                float z_ndc = view_to_projected_depth(view_depth, a.near_plane, a.far_plane);
+                depth = gmin(depth, z_ndc);
+                if (kDepthOnly) continue;
+                color.x += (float)((val >> 24) & 0xFFFu) / 255.0f;
+                color.y += (float)((val >> 12) & 0xFFFu) / 255.0f;
+                color.z += (float)((val >> 0) & 0xFFFu) / 255.0f;
+            }
+    float inv_passes = 1.0f / (float)(a.num_passes * a.ss * a.ss);
+    if (!kDepthOnly) {
+        a.color[3 * idx + 0] = color.x * inv_passes;
+        a.color[3 * idx + 1] = color.y * inv_passes;
+        a.color[3 * idx + 2] = color.z * inv_passes;
+    }
+    a.depth[idx] = depth;
+}
+
+// ---------------------------------------------------------------------------------
+// Hi-Z chain (depth_mip_chain.cu:7-67)
+// ---------------------------------------------------------------------------------
+__global__ void hiz_blit_kernel(HizView c, const float* __restrict__ src) {
+    const int l = c.levels - 1;
+    const int wl = c.level_w[l], hl = c.level_h[l];
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y * blockDim.y + threadIdx.y;
+    if (x >= wl || y >= hl) return;
+    c.mip[c.level_off[l] + (uint64_t)y * wl + x] = src[(uint64_t)y * wl + x];
+}
+
+template <bool kMin>
+__global__ void hiz_reduce_kernel(HizView c, int l) {
+    const int wl = c.level_w[l], hl = c.level_h[l];
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y * blockDim.y + threadIdx.y;
+    if (x >= wl || y >= hl) return;
+    const int wf = c.level_w[l + 1], hf = c.level_h[l + 1];
+    const float* fine = c.mip + c.level_off[l + 1];
+    float v = kMin ? INFINITY : -INFINITY;
+    for (int dy = 0; dy < 2; ++dy)
+        for (int dx = 0; dx < 2; ++dx) {
+            const int fx = 2 * x + dx, fy = 2 * y + dy;
+            if (fx < wf && fy < hf) {
+                float f = fine[(uint64_t)fy * wf + fx];
+                v = kMin ? fminf(v, f) : fmaxf(v, f);
+            }
+        }
+    c.mip[c.level_off[l] + (uint64_t)y * wl + x] = v;
+}
+
+// ---------------------------------------------------------------------------------
+// Block AABBs at load time (gaussian_bvh.cu:111-144).  The reference computes these on the
+// host in IEEE single precision without fused multiply-adds; the _rn intrinsics below keep
+// nvcc from contracting, so the boxes are bit-identical to the host computation.
+// ---------------------------------------------------------------------------------
+__device__ __forceinline__ float rmul(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ float radd(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ float rsub(float a, float b) { return __fsub_rn(a, b); }
+
+__device__ __forceinline__ void host_order_cov_diag(vec3 s, vec4 q, float out[3]) {
+    const float w = q.x, x = q.y, y = q.z, z = q.w;
+    float qxx = rmul(x, x), qyy = rmul(y, y), qzz = rmul(z, z);
+    float qxz = rmul(x, z), qxy = rmul(x, y), qyz = rmul(y, z);
+    float qwx = rmul(w, x), qwy = rmul(w, y), qwz = rmul(w, z);
+    float r[3][3];
+    r[0][0] = rsub(1.0f, rmul(2.0f, radd(qyy, qzz)));
+    r[0][1] = rmul(2.0f, radd(qxy, qwz));
+    r[0][2] = rmul(2.0f, rsub(qxz, qwy));
+    r[1][0] = rmul(2.0f, rsub(qxy, qwz));
+    r[1][1] = rsub(1.0f, rmul(2.0f, radd(qxx, qzz)));
+    r[1][2] = rmul(2.0f, radd(qyz, qwx));
+    r[2][0] = rmul(2.0f, radd(qxz, qwy));
+    r[2][1] = rmul(2.0f, rsub(qyz, qwx));
+    r[2][2] = rsub(1.0f, rmul(2.0f, radd(qxx, qyy)));
+    // M = R * S, column j = (R0*S[j].x + R1*S[j].y) + R2*S[j].z with S diagonal
+    float sd[3][3] = {{s.x, 0.0f, 0.0f}, {0.0f, s.y, 0.0f}, {0.0f, 0.0f, s.z}};
+    float m[3][3];
+    for (int j = 0; j < 3; ++j)
+        for (int i = 0; i < 3; ++i)
+            m[j][i] = radd(radd(rmul(r[0][i], sd[j][0]), rmul(r[1][i], sd[j][1])), rmul(r[2][i], sd[j][2]));
+    // cov = M * M^T: cov[j][i] = (M0[i]*M[0][j] + M1[i]*M[1][j]) + M2[i]*M[2][j]; diagonal only
+    for (int i = 0; i < 3; ++i)
+        out[i] = radd(radd(rmul(m[0][i], m[0][i]), rmul(m[1][i], m[1][i])), rmul(m[2][i], m[2][i]));
+}
+
+__global__ void block_bounds_kernel(const float4* __restrict__ pos_op, const float4* __restrict__ rot,
+                                    const float4* __restrict__ scale, uint32_t n, uint32_t per_block,
+                                    float4* __restrict__ nodes, uint32_t node_count) {
+    const uint32_t node = blockIdx.x * blockDim.x + threadIdx.x;
+    if (node >= node_count) return;
+    const uint32_t begin = node * per_block;
+    const uint32_t end = min(begin + per_block, n);
+    float bmin[3] = {3.402823466e+38f, 3.402823466e+38f, 3.402823466e+38f};
+    float bmax[3] = {-3.402823466e+38f, -3.402823466e+38f, -3.402823466e+38f};
+    for (uint32_t g = begin; g < end; ++g) {
+        float4 p = pos_op[g], q = rot[g], s = scale[g];
+        float d[3];
+        host_order_cov_diag(make_v3(s.x, s.y, s.z), make_v4(q.x, q.y, q.z, q.w), d);
+        float mean[3] = {p.x, p.y, p.z};
+        for (int i = 0; i < 3; ++i) {
+            float ext = rmul(kTruncationStd, __fsqrt_rn(d[i]));
+            float lo = rsub(mean[i], ext), hi = radd(mean[i], ext);
+            bmin[i] = (lo < bmin[i]) ? lo : bmin[i];
+            bmax[i] = (bmax[i] < hi) ? hi : bmax[i];
+        }
+    }
+    nodes[2 * node] = make_float4(bmin[0], bmin[1], bmin[2], __uint_as_float(begin));
+    nodes[2 * node + 1] = make_float4(bmax[0], bmax[1], bmax[2], __uint_as_float(end - begin));
+}
+
+// ---------------------------------------------------------------------------------
+// Post-processing (post_processing_kernels.cuh:108-285)
+// ---------------------------------------------------------------------------------
+__device__ __forceinline__ float mixf(float x, float y, float a) { return x * (1.0f - a) + y * a; }
+__device__ __forceinline__ vec3 mix3s(vec3 x, vec3 y, float a) {
+    return make_v3(mixf(x.x, y.x, a), mixf(x.y, y.y, a), mixf(x.z, y.z, a));
+}
+__device__ __forceinline__ vec3 ld3(const float* p, int i) { return make_v3(p[3 * i], p[3 * i + 1], p[3 * i + 2]); }
+
+// temporalRender reads the 3x3 neighbourhood of the current colour buffer while other threads
+// overwrite that same buffer with blended results, so its output depends on thread order.
+// Here the blended colour goes to a separate buffer (out_color, never aliasing cur_color): the
+// neighbourhood is always the unblended current frame and the result is deterministic.
+__global__ void taa_kernel(uint8_t* __restrict__ image, float* __restrict__ out_color,
+                           const float* __restrict__ cur_color,
+                           const float* __restrict__ prev_color, const float* __restrict__ cur_depth,
+                           const float* __restrict__ prev_depth, mat4 reproj, float blend, int width, int height,
+                           int frame_number) {
+    int idx = blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= width * height) return;
+    int x = idx % width;
+    int y = idx / width;
+    vec3 color = ld3(cur_color, idx);
+    float depth = cur_depth[idx];
+    if (frame_number > 0) {
+        vec4 clip = make_v4((x + 0.5f) / width * 2.0f - 1.0f, (y + 0.5f) / height * 2.0f - 1.0f, depth, 1.0f);
+        vec4 prev = reproj * clip;
+        prev = make_v4(prev.x / prev.w, prev.y / prev.w, prev.z / prev.w, prev.w / prev.w);
+        float px = (prev.x * 0.5f + 0.5f) * width - 0.5f;
+        float py = (prev.y * 0.5f + 0.5f) * height - 0.5f;
+        if (px >= 0 && px < width && py >= 0 && py < height) {
+            // bilinearSampleCombined
+            int x0 = (int)floorf(px), y0 = (int)floorf(py);
+            int x1 = x0 + 1, y1 = y0 + 1;
+            x0 = (x0 < 0) ? 0 : ((x0 >= width) ? width - 1 : x0);
+            y0 = (y0 < 0) ? 0 : ((y0 >= height) ? height - 1 : y0);
+            x1 = (x1 < 0) ? 0 : ((x1 >= width) ? width - 1 : x1);
+            y1 = (y1 < 0) ? 0 : ((y1 >= height) ? height - 1 : y1);
+            float tx = px - floorf(px);
+            float ty = py - floorf(py);
+            int i00 = y0 * width + x0, i10 = y0 * width + x1, i01 = y1 * width + x0, i11 = y1 * width + x1;
+            (void)prev_depth;
+            vec3 top = mix3s(ld3(prev_color, i00), ld3(prev_color, i10), tx);
+            vec3 bottom = mix3s(ld3(prev_color, i01), ld3(prev_color, i11), tx);
+            vec3 hist = mix3s(top, bottom, ty);
+            // computeNeighborhoodMinMax
+            vec3 nmin = make_v3(1e9f, 1e9f, 1e9f), nmax = make_v3(-1e9f, -1e9f, -1e9f);
+            for (int dy = -1; dy <= 1; dy++) {
+                int yy = y + dy;
+                if (yy < 0 || yy >= height) continue;
+                for (int dx = -1; dx <= 1; dx++) {
+                    int xx = x + dx;
+                    if (xx < 0 || xx >= width) continue;
+                    vec3 c = ld3(cur_color, yy * width + xx);
+                    nmin = make_v3(gmin(nmin.x, c.x), gmin(nmin.y, c.y), gmin(nmin.z, c.z));
+                    nmax = make_v3(gmax(nmax.x, c.x), gmax(nmax.y, c.y), gmax(nmax.z, c.z));
+                }
+            }
+            vec3 h = make_v3(gclamp(hist.x, nmin.x - 0.05f, nmax.x + 0.05f), gclamp(hist.y, nmin.y - 0.05f, nmax.y + 0.05f),
+                             gclamp(hist.z, nmin.z - 0.05f, nmax.z + 0.05f));
+            color = mix3s(color, h, blend);
+        }
+    }
+    out_color[3 * idx + 0] = color.x;
+    out_color[3 * idx + 1] = color.y;
+    out_color[3 * idx + 2] = color.z;
+    vec3 o = make_v3(gclamp(color.x, 0.0f, 1.0f) * 255.0f, gclamp(color.y, 0.0f, 1.0f) * 255.0f,
+                     gclamp(color.z, 0.0f, 1.0f) * 255.0f);
+    image[3 * idx + 0] = (uint8_t)roundf(o.x);
+    image[3 * idx + 1] = (uint8_t)roundf(o.y);
+    image[3 * idx + 2] = (uint8_t)roundf(o.z);
+}
+
+__global__ void progressive_kernel(uint8_t* __restrict__ image, float* __restrict__ cur, float* __restrict__ accum,
+                                   int width, int height, int frames) {
+    int idx = blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= width * height) return;
+    vec3 color = ld3(cur, idx);
+    if (frames > 1) color = color + ld3(accum, idx);
+    cur[3 * idx + 0] = color.x;
+    cur[3 * idx + 1] = color.y;
+    cur[3 * idx + 2] = color.z;
+    accum[3 * idx + 0] = 0.0f;
+    accum[3 * idx + 1] = 0.0f;
+    accum[3 * idx + 2] = 0.0f;
+    color = color * (255.0f / (float)frames);
+    color = make_v3(gclamp(color.x, 0.0f, 255.0f), gclamp(color.y, 0.0f, 255.0f), gclamp(color.z, 0.0f, 255.0f));
+    image[3 * idx + 0] = (uint8_t)roundf(color.x);
+    image[3 * idx + 1] = (uint8_t)roundf(color.y);
+    image[3 * idx + 2] = (uint8_t)roundf(color.z);
+}
+
+int g_num_sms = 0;
+int g_splat_blocks_per_sm = 0;
+
+}  // namespace
+
+// ---------------------------------------------------------------------------------
+// launchers
+// ---------------------------------------------------------------------------------
+void launch_block_cull(const BlockView& b, const FrameConst& fc, const HizView& hiz, cudaStream_t stream) {
+    if (b.node_count == 0) return;
+    uint32_t threads = b.words * 32;
+    block_cull_kernel<<<(threads + 255) / 256, 256, 0, stream>>>(b, fc, hiz);
+}
+
+void launch_preprocess_fp32(const PreprocessArgs& a, const SceneFP32& s, cudaStream_t stream) {
+    if (a.n == 0) return;
+    preprocess_kernel<SceneFP32><<<(a.n + 255) / 256, 256, 0, stream>>>(a, s);
+}
+
+void launch_preprocess_compressed(const PreprocessArgs& a, const SceneCompressed& s, cudaStream_t stream) {
+    if (a.n == 0) return;
+    preprocess_kernel<SceneCompressed><<<(a.n + 255) / 256, 256, 0, stream>>>(a, s);
+}
+
+uint32_t scan_tile_count(uint32_t n) { return (n + kScanTile - 1) / kScanTile; }
+
+void launch_scan(const ScanArgs& a, uint32_t scan_tiles, cudaStream_t stream) {
+    cudaMemsetAsync(a.tile_state, 0, sizeof(unsigned long long) * scan_tiles, stream);
+    cudaMemsetAsync(a.tile_ticket, 0, sizeof(uint32_t), stream);
+    cudaMemsetAsync(a.counters, 0, sizeof(PassCounters), stream);
+    if (scan_tiles == 0) return;
+    scan_kernel<<<scan_tiles, kScanThreads, 0, stream>>>(a);
+}
+
+int splat_grid_size(int block) {
+    if (g_num_sms == 0) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&g_num_sms, cudaDevAttrMultiProcessorCount, dev);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&g_splat_blocks_per_sm, splat_kernel, block, 0);
+        if (g_splat_blocks_per_sm < 1) g_splat_blocks_per_sm = 1;
+    }
+    return g_num_sms * g_splat_blocks_per_sm;
+}
+
+void launch_splat(const SplatArgs& a, int grid, int block, cudaStream_t stream) {
+    (void)block;
+    splat_kernel<<<grid, kSplatTile, 0, stream>>>(a);
+}
+
+void launch_clear(uint64_t* buf, uint64_t entries, uint64_t value, cudaStream_t stream) {
+    uint64_t pairs = entries / 2;
+    int grid = (int)((pairs + 255) / 256);
+    if (grid > 148 * 16) grid = 148 * 16;
+    if (grid < 1) grid = 1;
+    clear_kernel<<<grid, 256, 0, stream>>>(reinterpret_cast<ulonglong2*>(buf), pairs, value);
+    if (entries & 1) cudaMemcpyAsync(buf + entries - 1, &buf[0], 8, cudaMemcpyDeviceToDevice, stream);
+}
+
+void launch_resolve(const ResolveArgs& a, bool depth_only, cudaStream_t stream) {
+    dim3 block(16, 16);
+    dim3 grid((a.width + 15) / 16, (a.height + 15) / 16);
+    if (depth_only) resolve_kernel<true><<<grid, block, 0, stream>>>(a);
+    else resolve_kernel<false><<<grid, block, 0, stream>>>(a);
+}
+
+void launch_hiz_build(const HizView& h, const float* depth, int min_levels, cudaStream_t stream) {
+    dim3 block(16, 16);
+    {
+        const int l = h.levels - 1;
+        dim3 grid((h.level_w[l] + 15) / 16, (h.level_h[l] + 15) / 16);
+        hiz_blit_kernel<<<grid, block, 0, stream>>>(h, depth);
+    }
+    for (int l = h.levels - 2; l >= 0; --l) {
+        dim3 grid((h.level_w[l] + 15) / 16, (h.level_h[l] + 15) / 16);
+        int from_finest = (h.levels - 2) - l;
+        if (from_finest < min_levels) hiz_reduce_kernel<true><<<grid, block, 0, stream>>>(h, l);
+        else hiz_reduce_kernel<false><<<grid, block, 0, stream>>>(h, l);
+    }
+}
+
+void launch_block_bounds(const float4* pos_op, const float4* rot, const float4* scale, uint32_t n,
+                         uint32_t per_block, float4* nodes, cudaStream_t stream) {
+    uint32_t node_count = (n + per_block - 1) / per_block;
+    if (node_count == 0) return;
+    block_bounds_kernel<<<(node_count + 255) / 256, 256, 0, stream>>>(pos_op, rot, scale, n, per_block, nodes,
+                                                                       node_count);
+}
+
+void launch_taa(uint8_t* image, float* out_color, const float* cur_color, const float* prev_color,
+                const float* cur_depth, const float* prev_depth, const mat4& reproj, float blend, int width, int height,
+                int frame_number, cudaStream_t stream) {
+    int n = width * height;
+    taa_kernel<<<(n + 255) / 256, 256, 0, stream>>>(image, out_color, cur_color, prev_color, cur_depth, prev_depth,
+                                                     reproj, blend, width, height, frame_number);
+}
+
+void launch_progressive(uint8_t* image, float* cur_color, float* accum, int width, int height, int frames,
+                        cudaStream_t stream) {
+    int n = width * height;
+    progressive_kernel<<<(n + 255) / 256, 256, 0, stream>>>(image, cur_color, accum, width, height, frames);
+}
+
+}  // namespace gps

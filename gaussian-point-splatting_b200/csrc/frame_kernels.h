@@ -1,0 +1,136 @@
+// Internal interface between the frame driver (renderer.cu) and the sm_100a kernels
+// (frame_kernels.cu).  Nothing here crosses the C-ABI.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+#include "gps_math.cuh"
+#include "gps_scene.cuh"
+
+namespace gps {
+
+// Per-surviving-Gaussian data the splat needs, produced once by the preprocess (the
+// reference recomputes this per point, gaussian_point_splatting.cu:416-423).  64 bytes:
+//   a = (pixel_mean.x, pixel_mean.y, c0, c1)   Cholesky factor of cov2d
+//   b = (c2, conic.x, conic.y, conic.z)
+//   c = (opacity, colour.r, colour.g, colour.b) colour is the SH evaluation of this frame
+//   d = (min.x | min.y << 16, max.x | max.y << 16, key.lo, key.hi)  key = depth28<<36 | rgb36
+struct SplatRecord {
+    float4 a, b, c;
+    uint4 d;
+};
+
+// Hi-Z max-depth pyramid layout (depth_mip_chain.cuh:10-71).
+struct HizView {
+    float* mip;
+    int width, height, levels;
+    uint64_t mip_size;
+    int level_w[16];
+    int level_h[16];
+    uint64_t level_off[16];
+};
+
+// Fixed-size contiguous Gaussian blocks with AABBs (gaussian_bvh.cuh:8-53).
+struct BlockView {
+    const float4* nodes;   // 2 float4 per node: (min.xyz, begin bits), (max.xyz, count bits)
+    uint32_t* culled;      // one bit per node, 32 nodes per word
+    uint32_t node_count;
+    uint32_t words;
+    uint32_t per_block;    // Gaussians per block
+};
+
+// Device-side counters of one render pass, readable by later kernels without a host sync.
+struct PassCounters {
+    uint32_t survivors;    // Gaussians with at least one point
+    uint32_t total_points; // sum of point counts (u32, wraps like the reference)
+    uint32_t points;       // min(total_points, max_number_of_points)
+    uint32_t truncated;    // 1 if the point budget clipped the tail
+    uint32_t scan_timeouts;
+    uint32_t pad[3];
+};
+
+struct FrameConst {
+    mat4 vp, view, cam;
+    vec2 tan_fov, focal;
+    int up_width, up_height;
+    int num_passes;        // samples per pixel
+    int ss;                // supersampling factor
+    int k_points;          // points per thread in the splat (ss*ss or 1)
+    float near_plane, far_plane;
+    vec4 planes[6];
+    int use_unbiased;
+    int reduce_point_count;
+    int cull_small;
+    int enable_occlusion;
+    int enable_hier;
+    int width, height;
+};
+
+struct PreprocessArgs {
+    FrameConst fc;
+    int frame_seed;
+    int only_previously_occluded;
+    uint32_t n;
+    uint32_t* counts;
+    uint32_t* mask_cur;
+    const uint32_t* mask_prev;
+    SplatRecord* records;
+    HizView hiz;
+    BlockView blocks;
+};
+
+struct ScanArgs {
+    const uint32_t* counts;
+    const uint32_t* mask;
+    uint32_t n;
+    uint32_t max_points;
+    uint32_t tile_points;        // points per splat tile
+    uint32_t* surv_gid;          // [n] compacted Gaussian ids of survivors
+    uint32_t* surv_start;        // [n] first point of each survivor
+    uint32_t* tile_first_rank;   // [ceil(max_points / tile_points) + 1]
+    unsigned long long* tile_state;  // [scan tiles] decoupled look-back status words
+    uint32_t* tile_ticket;       // dynamic tile counter
+    PassCounters* counters;
+};
+
+struct SplatArgs {
+    FrameConst fc;
+    int frame_seed;
+    const SplatRecord* records;
+    const uint32_t* surv_gid;
+    const uint32_t* surv_start;
+    const uint32_t* tile_first_rank;
+    const PassCounters* counters;
+    uint64_t* buffer;
+    uint32_t n;
+};
+
+struct ResolveArgs {
+    const uint64_t* buffer;
+    float* color;          // float3 per pixel (may be null for depth-only)
+    float* depth;
+    int width, height, num_passes, ss;
+    uint64_t entries;
+    float near_plane, far_plane;
+    uint64_t initial_value;
+};
+
+// launchers (all asynchronous on `stream`)
+void launch_block_cull(const BlockView& b, const FrameConst& fc, const HizView& hiz, cudaStream_t stream);
+void launch_preprocess_fp32(const PreprocessArgs& a, const SceneFP32& s, cudaStream_t stream);
+void launch_preprocess_compressed(const PreprocessArgs& a, const SceneCompressed& s, cudaStream_t stream);
+void launch_scan(const ScanArgs& a, uint32_t scan_tiles, cudaStream_t stream);
+uint32_t scan_tile_count(uint32_t n);
+void launch_splat(const SplatArgs& a, int grid, int block, cudaStream_t stream);
+void launch_clear(uint64_t* buf, uint64_t entries, uint64_t value, cudaStream_t stream);
+void launch_resolve(const ResolveArgs& a, bool depth_only, cudaStream_t stream);
+void launch_hiz_build(const HizView& h, const float* depth, int min_levels, cudaStream_t stream);
+void launch_block_bounds(const float4* pos_op, const float4* rot, const float4* scale, uint32_t n,
+                         uint32_t per_block, float4* nodes, cudaStream_t stream);
+void launch_taa(uint8_t* image, float* out_color, const float* cur_color, const float* prev_color,
+                const float* cur_depth, const float* prev_depth, const mat4& reproj, float blend, int width, int height,
+                int frame_number, cudaStream_t stream);
+void launch_progressive(uint8_t* image, float* cur_color, float* accum, int width, int height, int frames,
+                        cudaStream_t stream);
+int splat_grid_size(int block);
+
+}  // namespace gps

@@ -1,0 +1,258 @@
+// Device-resident Gaussian scene formats and their per-Gaussian accessors.
+//
+//   SceneFP32       — the reference's GPUGaussianSceneUncompressed
+//                     (src/core/gaussians/gaussian_types.cuh:548-646), stored here as
+//                     16-byte-aligned structure-of-arrays so that every attribute is fetched
+//                     with 128-bit loads: pos_op = (mean.xyz, opacity), rot = (w,x,y,z),
+//                     scale = (sx,sy,sz,0), sh = 12 float4 (48 interleaved RGB coefficients).
+//   SceneCompressed — the reference's default GPUGaussianSceneCompressed
+//                     (gaussian_types.cuh:173-374,421-541): 16-byte quantised geometry,
+//                     u8 opacity, compact SH (FP32 DC + 45 u8 AC, scene-wide min/max).
+//
+// Accessors return exactly the values the reference accessors return; the colour
+// evaluation follows sh.cuh:191-223 (FP32) and sh.cuh:41-47,55-96,257-273 (compact).
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+#include "gps_math.cuh"
+
+namespace gps {
+
+// GaussianSceneBounds (gaussian_types.cuh:127-171), the dequantisation ranges.
+struct SceneBounds {
+    vec3 min_pos, max_pos;
+    vec3 min_scale, max_scale;  // log-encoded
+    vec3 min_sh[15], max_sh[15];
+};
+
+constexpr float kShC0 = 0.28209479177387814f;
+constexpr float kShC1 = 0.4886025119029199f;
+
+#if defined(__CUDACC__)
+
+GPS_D vec3 normalize(vec3 v) { return v * (1.0f / sqrtf(dot(v, v))); }
+GPS_D vec3 vmax0(vec3 v) { return make_v3(gmax(v.x, 0.0f), gmax(v.y, 0.0f), gmax(v.z, 0.0f)); }
+
+// sh.cuh:191-223 with deg = 3 (the preprocess asks for degree 4, which evaluates all bands)
+GPS_D vec3 color_from_sh_fp32(vec3 pos, vec3 campos, const float* shs) {
+    vec3 dir = pos - campos;
+    dir = normalize(dir);
+#define GPS_SH(i) make_v3(shs[3 * (i)], shs[3 * (i) + 1], shs[3 * (i) + 2])
+    vec3 result = kShC0 * GPS_SH(0);
+    float x = dir.x, y = dir.y, z = dir.z;
+    result = result - kShC1 * y * GPS_SH(1) + kShC1 * z * GPS_SH(2) - kShC1 * x * GPS_SH(3);
+    float xx = x * x, yy = y * y, zz = z * z;
+    float xy = x * y, yz = y * z, xz = x * z;
+    result = result + (1.0925484305920792f * xy * GPS_SH(4) + -1.0925484305920792f * yz * GPS_SH(5) +
+                       0.31539156525252005f * (2.0f * zz - xx - yy) * GPS_SH(6) +
+                       -1.0925484305920792f * xz * GPS_SH(7) + 0.5462742152960396f * (xx - yy) * GPS_SH(8));
+    result = result + (-0.5900435899266435f * y * (3.0f * xx - yy) * GPS_SH(9) +
+                       2.890611442640554f * xy * z * GPS_SH(10) +
+                       -0.4570457994644658f * y * (4.0f * zz - xx - yy) * GPS_SH(11) +
+                       0.3731763325901154f * z * (2.0f * zz - 3.0f * xx - 3.0f * yy) * GPS_SH(12) +
+                       -0.4570457994644658f * x * (4.0f * zz - xx - yy) * GPS_SH(13) +
+                       1.445305721320277f * z * (xx - yy) * GPS_SH(14) +
+                       -0.5900435899266435f * x * (xx - 3.0f * yy) * GPS_SH(15));
+#undef GPS_SH
+    result = result + make_v3(0.5f, 0.5f, 0.5f);
+    return vmax0(result);
+}
+
+// a*b - c*d and a*b + c*d of the SH band recurrence with an explicit fused product
+#ifndef GPS_SH_FORM
+#define GPS_SH_FORM 32
+#endif
+GPS_D float sh_rec(float a, float b, float c, float d, bool minus, int bit) {
+    const float cd = minus ? -c : c;
+    if ((GPS_SH_FORM >> 5) & 1) return minus ? a * b - c * d : a * b + c * d;
+    if ((GPS_SH_FORM >> bit) & 1) return __fmaf_rn(cd, d, __fmul_rn(a, b));
+    return __fmaf_rn(a, b, __fmul_rn(cd, d));
+}
+
+// sh.cuh:55-96: real SH basis to band 3, Sloan's recurrence ordering
+GPS_D void eval_sh_basis_l3(float out[16], vec3 dir) {
+    float x, y, z, z2, c0, s0, c1, s1, d, a, b;
+    x = dir.x;
+    y = dir.y;
+    z = dir.z;
+    z2 = z * z;
+    d = 0.282094792f;
+    out[0] = d;
+    d = 0.488602512f * z;
+    out[2] = d;
+    a = z2 - 0.333333333f;
+    d = 0.946174696f * a;
+    out[6] = d;
+    b = z * (a - 0.266666667f);
+    d = 1.865881663f * b;
+    out[12] = d;
+    c1 = x;
+    s1 = y;
+    d = -0.488602512f;
+    out[1] = s1 * d;
+    out[3] = c1 * d;
+    d = -1.092548431f * z;
+    out[5] = s1 * d;
+    out[7] = c1 * d;
+    a = z2 - 0.2f;
+    d = -2.285228997f * a;
+    out[11] = s1 * d;
+    out[13] = c1 * d;
+    c0 = sh_rec(x, c1, y, s1, true, 1);
+    s0 = sh_rec(y, c1, x, s1, false, 2);
+    d = 0.546274215f;
+    out[4] = s0 * d;
+    out[8] = c0 * d;
+    d = 1.445305721f * z;
+    out[10] = s0 * d;
+    out[14] = c0 * d;
+    c1 = sh_rec(x, c0, y, s0, true, 3);
+    s1 = sh_rec(y, c0, x, s0, false, 4);
+    d = -0.59004359f;
+    out[9] = s1 * d;
+    out[15] = c1 * d;
+}
+
+// glm::mix(x, y, a) = x*(1-a) + y*a, per component.  Which of the two products nvcc fuses
+// into the multiply-add depends on the surrounding code, so the form is spelled out.
+#ifndef GPS_MIX_SITES
+#define GPS_MIX_SITES 0
+#endif
+template <int kSite>
+GPS_D float mixf_ref(float x, float y, float a) {
+    if ((GPS_MIX_SITES >> kSite) & 1) return __fmaf_rn(y, a, __fmul_rn(x, 1.0f - a));
+    return __fmaf_rn(x, 1.0f - a, __fmul_rn(y, a));
+}
+template <int kSite>
+GPS_D vec3 mix3(vec3 x, vec3 y, vec3 a) {
+    return make_v3(mixf_ref<kSite>(x.x, y.x, a.x), mixf_ref<kSite>(x.y, y.y, a.y), mixf_ref<kSite>(x.z, y.z, a.z));
+}
+
+#endif  // __CUDACC__
+
+struct SceneFP32 {
+    const float4* __restrict__ pos_op;
+    const float4* __restrict__ rot;
+    const float4* __restrict__ scale;
+    const float4* __restrict__ sh;
+    uint32_t n;
+
+#if defined(__CUDACC__)
+    GPS_D float opacity(uint32_t g) const {
+        return gmin(__ldg(&pos_op[g]).w, kMaxOpacity);
+    }
+    GPS_D void geometry(uint32_t g, vec3& mean, vec4& quat, vec3& s) const {
+        float4 a = __ldg(&pos_op[g]);
+        float4 q = __ldg(&rot[g]);
+        float4 c = __ldg(&scale[g]);
+        mean = make_v3(a.x, a.y, a.z);
+        quat = make_v4(q.x, q.y, q.z, q.w);
+        s = make_v3(c.x, c.y, c.z);
+    }
+    GPS_D vec3 color(uint32_t g, vec3 mean, vec3 campos) const {
+        float shs[48];
+        const float4* src = sh + (size_t)g * 12;
+#pragma unroll
+        for (int i = 0; i < 12; ++i) {
+            float4 v = __ldg(&src[i]);
+            shs[4 * i + 0] = v.x;
+            shs[4 * i + 1] = v.y;
+            shs[4 * i + 2] = v.z;
+            shs[4 * i + 3] = v.w;
+        }
+        return color_from_sh_fp32(mean, campos, shs);
+    }
+#endif
+};
+
+// Quantised geometry words (gaussian_types.cuh:173-181) + u8 opacity + compact SH.
+// Compact SH is stored as two arrays: dc (float4: DC rgb, unused lane) and ac (3 x uint4 =
+// 48 bytes holding the 45 AC bytes in the reference's order, 3 trailing pad bytes).
+struct SceneCompressed {
+    const uint4* __restrict__ geom;
+    const uint8_t* __restrict__ opac;
+    const float4* __restrict__ sh_dc;
+    const uint4* __restrict__ sh_ac;
+    SceneBounds bounds;
+    uint32_t n;
+
+#if defined(__CUDACC__)
+    GPS_D float opacity(uint32_t g) const {
+        return gmin((float)__ldg(&opac[g]) / 255.0f, kMaxOpacity);
+    }
+    // gaussian_types.cuh:322-374
+    GPS_D void geometry(uint32_t g, vec3& mean, vec4& quat, vec3& s) const {
+        uint4 q = __ldg(&geom[g]);
+        uint32_t px = q.x & 0x7FFFFFu;
+        uint32_t py_low9 = (q.x >> 23) & 0x1FFu;
+        uint32_t py_high13 = q.y & 0x1FFFu;
+        uint32_t pz_low19 = (q.y >> 13) & 0x7FFFFu;
+        uint32_t pz_high4 = q.z & 0xFu;
+        uint32_t py = py_low9 | (py_high13 << 9);
+        uint32_t pz = pz_low19 | (pz_high4 << 19);
+        float fx = float(px) / float((1u << 23) - 1u);
+        float fy = float(py) / float((1u << 22) - 1u);
+        float fz = float(pz) / float((1u << 23) - 1u);
+        mean = mix3<0>(bounds.min_pos, bounds.max_pos, make_v3(fx, fy, fz));
+
+        uint32_t rx = (q.z >> 4) & 0x3FFu;
+        uint32_t ry = (q.z >> 14) & 0x3FFu;
+        uint32_t rz_low8 = (q.z >> 24) & 0xFFu;
+        uint32_t rz_high2 = q.w & 0x3u;
+        uint32_t rz = rz_low8 | (rz_high2 << 8);
+        vec3 vr = make_v3((float)rx / 1023.0f, (float)ry / 1023.0f, (float)rz / 1023.0f);
+        vec3 v = make_v3(vr.x * 2.0f - 1.0f, vr.y * 2.0f - 1.0f, vr.z * 2.0f - 1.0f);
+        // quat_iem (gaussian_types.cuh:215-235), device branch
+        float d = v.x * v.x + v.y * v.y + v.z * v.z;
+        float t = rsqrtf(d + 1e-8f);
+        float a = 1.57079632679f * t * d;
+        float sn = __sinf(a);
+        float cs = __cosf(a);
+        float k = sn * t;
+        quat = make_v4(k * v.x, k * v.y, k * v.z, cs);
+
+        uint32_t sx = (q.w >> 2) & 0x3FFu;
+        uint32_t sy = (q.w >> 12) & 0x3FFu;
+        uint32_t sz = (q.w >> 22) & 0x3FFu;
+        vec3 st = make_v3((float)sx / 1023.0f, (float)sy / 1023.0f, (float)sz / 1023.0f);
+        vec3 ls = mix3<1>(bounds.min_scale, bounds.max_scale, st);
+        s = make_v3(__expf(ls.x), __expf(ls.y), __expf(ls.z));
+    }
+    // sh.cuh:257-273 with CompactSH::get (sh.cuh:41-47)
+    GPS_D vec3 color(uint32_t g, vec3 mean, vec3 campos) const {
+        vec3 dir = mean - campos;
+        dir = normalize(dir);
+        float e[16];
+        eval_sh_basis_l3(e, dir);
+        float4 dc = __ldg(&sh_dc[g]);
+        uint32_t w[12];
+        const uint4* src = sh_ac + (size_t)g * 3;
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+            uint4 u = __ldg(&src[i]);
+            w[4 * i + 0] = u.x;
+            w[4 * i + 1] = u.y;
+            w[4 * i + 2] = u.z;
+            w[4 * i + 3] = u.w;
+        }
+        vec3 result = make_v3(0.0f, 0.0f, 0.0f);
+        result = result + e[0] * make_v3(dc.x, dc.y, dc.z);
+#pragma unroll
+        for (int i = 1; i < 16; ++i) {
+            const int j = i - 1;
+            const float r = 1.0f / 255.0f;
+            int b0 = 3 * j, b1 = 3 * j + 1, b2 = 3 * j + 2;
+            uint32_t q0 = (w[b0 >> 2] >> (8 * (b0 & 3))) & 0xFFu;
+            uint32_t q1 = (w[b1 >> 2] >> (8 * (b1 & 3))) & 0xFFu;
+            uint32_t q2 = (w[b2 >> 2] >> (8 * (b2 & 3))) & 0xFFu;
+            vec3 vq = make_v3((float)(int)q0 * r, (float)(int)q1 * r, (float)(int)q2 * r);
+            vec3 c = mix3<2>(bounds.min_sh[j], bounds.max_sh[j], vq);
+            result = result + e[i] * c;
+        }
+        result = result + make_v3(0.5f, 0.5f, 0.5f);
+        return vmax0(result);
+    }
+#endif
+};
+
+}  // namespace gps

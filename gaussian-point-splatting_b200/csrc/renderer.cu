@@ -1,0 +1,976 @@
+// Frame driver and C-ABI of the B200-native Gaussian point-splatting path.
+//
+// gps_render_frame reproduces GaussianPointSplatting::render
+// (src/core/rendering/passes/gaussian_point_splatting.cu:599-737): clear, pass 1 (block
+// cull -> preprocess -> scan -> splat), optionally depth-only resolve -> Hi-Z -> pass 2 over
+// the Gaussians that did not splat in pass 1, final resolve, Hi-Z for the next frame.
+// Unlike the reference it performs no host synchronisation and no allocation per frame:
+// the point count P stays on the device (the splat kernel reads it), so the whole frame is
+// a fixed sequence of asynchronous launches on the caller's stream.
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+#include "../../include/gps_b200.h"
+#include "frame_kernels.h"
+#include "host_io.hpp"
+
+using namespace gps;
+
+namespace {
+
+struct CudaError : std::exception {
+    std::string msg;
+    explicit CudaError(std::string m) : msg(std::move(m)) {}
+    const char* what() const noexcept override { return msg.c_str(); }
+};
+
+#define GPS_CUDA(call)                                                                              \
+    do {                                                                                            \
+        cudaError_t e_ = (call);                                                                    \
+        if (e_ != cudaSuccess) throw CudaError(std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+template <class T>
+T* dev_alloc(size_t count) {
+    if (count == 0) count = 1;
+    void* p = nullptr;
+    cudaError_t e = cudaMalloc(&p, count * sizeof(T));
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        throw CudaError(std::string("cudaMalloc of ") + std::to_string(count * sizeof(T)) + " bytes: " + cudaGetErrorString(e));
+    }
+    return static_cast<T*>(p);
+}
+
+struct DevFree {
+    void operator()(void* p) const {
+        if (p) cudaFree(p);
+    }
+};
+template <class T>
+using dptr = std::unique_ptr<T, DevFree>;
+
+gps_status fail(gps_status s, const std::string& msg) {
+    set_last_error(msg);
+    return s;
+}
+
+cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }
+
+mat4 mat4_from(const float* m) {
+    mat4 r;
+    for (int c = 0; c < 4; ++c) r.c[c] = make_v4(m[4 * c], m[4 * c + 1], m[4 * c + 2], m[4 * c + 3]);
+    return r;
+}
+void mat4_to(const mat4& m, float* out) {
+    for (int c = 0; c < 4; ++c) {
+        out[4 * c] = m.c[c].x;
+        out[4 * c + 1] = m.c[c].y;
+        out[4 * c + 2] = m.c[c].z;
+        out[4 * c + 3] = m.c[c].w;
+    }
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------------
+// scene
+// ---------------------------------------------------------------------------------
+struct gps_scene {
+    int format = GPS_SCENE_FP32;
+    uint64_t n = 0;
+    bool presorted = false;
+    // FP32 arrays (FP32 format)
+    dptr<float4> pos_op, rot, scale, sh;
+    // compressed arrays
+    dptr<uint4> geom, sh_ac;
+    dptr<uint8_t> opac;
+    dptr<float4> sh_dc;
+    SceneBounds bounds{};
+    // fixed-size blocks for the hierarchical cull (computed from the FP32 values, like
+    // build_fixed_blocks on the host CPUGaussian array)
+    dptr<float4> block_nodes;
+    uint32_t per_block = 4;
+    uint32_t block_count = 0;
+};
+
+namespace {
+
+void scene_upload(gps_scene* s, const CpuGaussian* g, uint64_t n) {
+    s->n = n;
+    s->per_block = gaussians_per_block(n);
+    s->block_count = (uint32_t)((n + s->per_block - 1) / s->per_block);
+    // repack into 16-byte SoA in chunks through pinned staging
+    const uint64_t chunk = 1u << 20;
+    float4* stage = nullptr;
+    GPS_CUDA(cudaMallocHost(&stage, chunk * sizeof(float4) * 15));
+    std::unique_ptr<float4, void (*)(float4*)> stage_guard(stage, [](float4* p) { cudaFreeHost(p); });
+    float4* d_pos = dev_alloc<float4>(n);
+    s->pos_op.reset(d_pos);
+    float4* d_rot = dev_alloc<float4>(n);
+    s->rot.reset(d_rot);
+    float4* d_scale = dev_alloc<float4>(n);
+    s->scale.reset(d_scale);
+    float4* d_sh = nullptr;
+    if (s->format == GPS_SCENE_FP32) {
+        d_sh = dev_alloc<float4>(n * 12);
+        s->sh.reset(d_sh);
+    }
+    for (uint64_t b = 0; b < n; b += chunk) {
+        uint64_t e = std::min(n, b + chunk), m = e - b;
+        float4* sp = stage;
+        float4* sr = stage + chunk;
+        float4* ss = stage + 2 * chunk;
+        float4* sh = stage + 3 * chunk;
+        for (uint64_t i = 0; i < m; ++i) {
+            const CpuGaussian& q = g[b + i];
+            sp[i] = make_float4(q.mean[0], q.mean[1], q.mean[2], q.opacity);
+            sr[i] = make_float4(q.rot[0], q.rot[1], q.rot[2], q.rot[3]);
+            ss[i] = make_float4(q.scale[0], q.scale[1], q.scale[2], 0.0f);
+            if (d_sh) std::memcpy(sh + i * 12, q.sh, sizeof(float) * 48);
+        }
+        GPS_CUDA(cudaMemcpy(d_pos + b, sp, m * sizeof(float4), cudaMemcpyHostToDevice));
+        GPS_CUDA(cudaMemcpy(d_rot + b, sr, m * sizeof(float4), cudaMemcpyHostToDevice));
+        GPS_CUDA(cudaMemcpy(d_scale + b, ss, m * sizeof(float4), cudaMemcpyHostToDevice));
+        if (d_sh) GPS_CUDA(cudaMemcpy(d_sh + b * 12, sh, m * 12 * sizeof(float4), cudaMemcpyHostToDevice));
+    }
+    float4* nodes = dev_alloc<float4>((size_t)s->block_count * 2);
+    s->block_nodes.reset(nodes);
+    launch_block_bounds(d_pos, d_rot, d_scale, (uint32_t)n, s->per_block, nodes, 0);
+    GPS_CUDA(cudaGetLastError());
+    if (s->format == GPS_SCENE_COMPRESSED) {
+        s->bounds = compute_scene_bounds(g, n);
+        std::vector<uint4> geom(n), ac(n * 3);
+        std::vector<uint8_t> op(n);
+        std::vector<float4> dc(n);
+        encode_compressed(g, n, s->bounds, geom.data(), op.data(), dc.data(), ac.data());
+        s->geom.reset(dev_alloc<uint4>(n));
+        s->sh_ac.reset(dev_alloc<uint4>(n * 3));
+        s->opac.reset(dev_alloc<uint8_t>(n));
+        s->sh_dc.reset(dev_alloc<float4>(n));
+        GPS_CUDA(cudaMemcpy(s->geom.get(), geom.data(), n * sizeof(uint4), cudaMemcpyHostToDevice));
+        GPS_CUDA(cudaMemcpy(s->sh_ac.get(), ac.data(), n * 3 * sizeof(uint4), cudaMemcpyHostToDevice));
+        GPS_CUDA(cudaMemcpy(s->opac.get(), op.data(), n, cudaMemcpyHostToDevice));
+        GPS_CUDA(cudaMemcpy(s->sh_dc.get(), dc.data(), n * sizeof(float4), cudaMemcpyHostToDevice));
+        GPS_CUDA(cudaDeviceSynchronize());
+        // the compressed renderer needs no FP32 geometry once the blocks exist
+        s->pos_op.reset();
+        s->rot.reset();
+        s->scale.reset();
+    }
+    GPS_CUDA(cudaDeviceSynchronize());
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------------
+// renderer
+// ---------------------------------------------------------------------------------
+// Optional per-stage timing: CUDA events recorded between the stages of each frame on the
+// frame's own stream; intervals are accumulated when read (or when the event pool fills).
+enum Stage { kStClear, kStCull, kStPreprocess, kStScan, kStSplat, kStResolve, kStHiz, kStPost, kStCount };
+
+struct StageTimer {
+    bool on = false;
+    std::vector<cudaEvent_t> pool;
+    std::vector<int> stage;  // stage that starts at event i (-1: frame end)
+    size_t used = 0;
+    double total_ms[kStCount] = {0};
+    uint64_t launches[kStCount] = {0};
+    int frames = 0;
+    ~StageTimer() {
+        for (auto e : pool) cudaEventDestroy(e);
+    }
+    void drain() {
+        if (used == 0) return;
+        cudaEventSynchronize(pool[used - 1]);
+        for (size_t i = 0; i + 1 < used; ++i) {
+            if (stage[i] < 0) continue;
+            float ms = 0.0f;
+            if (cudaEventElapsedTime(&ms, pool[i], pool[i + 1]) == cudaSuccess) total_ms[stage[i]] += ms;
+        }
+        used = 0;
+    }
+    void mark(int st, cudaStream_t s) {
+        if (!on) return;
+        if (used == pool.size()) {
+            // keep the last event as the start of the next interval
+            cudaEvent_t last = pool[used - 1];
+            int last_stage = stage[used - 1];
+            drain();
+            std::swap(pool[0], pool[pool.size() - 1]);
+            (void)last;
+            stage[0] = last_stage;
+            used = 1;
+        }
+        stage[used] = st;
+        cudaEventRecord(pool[used], s);
+        ++used;
+    }
+};
+
+struct gps_renderer {
+    StageTimer timer;
+    uint64_t frame_launches = 0;  // kernels launched by the last frame
+    gps_scene* scene = nullptr;
+    gps_settings s{};
+    int up_w = 0, up_h = 0;
+    uint64_t entries = 0;
+    uint32_t n = 0, n_pad = 0;
+    dptr<uint64_t> buffer;
+    dptr<uint32_t> counts, mask[2], surv_gid, surv_start, tile_first_rank, ticket, culled;
+    dptr<SplatRecord> records;
+    dptr<unsigned long long> tile_state;
+    dptr<PassCounters> counters;  // [2]: pass 1, pass 2
+    dptr<float> mip;
+    HizView hiz{};
+    uint32_t scan_tiles = 0;
+    uint32_t iteration = 0;
+    int splat_grid = 0;
+    PassCounters* host_counters = nullptr;  // pinned [2]
+    cudaEvent_t done = nullptr;
+    bool have_frame = false;
+    bool second_pass_last = false;
+    ~gps_renderer() {
+        if (host_counters) cudaFreeHost(host_counters);
+        if (done) cudaEventDestroy(done);
+    }
+};
+
+namespace {
+
+void hiz_layout(HizView& h, int w, int hgt) {
+    h.width = w;
+    h.height = hgt;
+    int max_dim = std::max(w, hgt), e = 0;
+    while ((1 << e) < max_dim) ++e;
+    h.levels = e + 1;
+    uint64_t off = 0;
+    for (int l = 0; l < h.levels; ++l) {
+        int fe = h.levels - 1;
+        h.level_w[l] = std::max(1, (w + (1 << (fe - l)) - 1) >> (fe - l));
+        h.level_h[l] = std::max(1, (hgt + (1 << (fe - l)) - 1) >> (fe - l));
+        h.level_off[l] = off;
+        off += (uint64_t)h.level_w[l] * (uint64_t)h.level_h[l];
+    }
+    h.mip_size = off;
+}
+
+__global__ void fill_f32(float* p, uint64_t n, float v) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) p[i] = v;
+}
+
+FrameConst make_frame_const(const gps_renderer* r, const gps_camera* cam) {
+    FrameConst fc{};
+    mat4 view = mat4_from(cam->view), proj = mat4_from(cam->proj);
+    mat4 vp, cm;
+    vec2 tan_fov, focal;
+    derive_frame(view, proj, r->s.width, r->s.height, r->s.supersampling_factor, r->s.fovy, vp, cm, tan_fov, focal);
+    fc.vp = vp;
+    fc.view = view;
+    fc.cam = cm;
+    fc.tan_fov = tan_fov;
+    fc.focal = focal;
+    fc.up_width = r->up_w;
+    fc.up_height = r->up_h;
+    fc.num_passes = r->s.samples_per_pixel;
+    fc.ss = r->s.supersampling_factor;
+    fc.k_points = r->s.reduce_point_count ? fc.ss * fc.ss * kPointsPerKernel : 1;
+    fc.near_plane = r->s.near_view_plane;
+    fc.far_plane = r->s.far_view_plane;
+    for (int i = 0; i < 6; ++i)
+        fc.planes[i] = make_v4(cam->frustum_planes[4 * i], cam->frustum_planes[4 * i + 1], cam->frustum_planes[4 * i + 2],
+                               cam->frustum_planes[4 * i + 3]);
+    fc.use_unbiased = r->s.use_unbiased_2d_splatting ? 1 : 0;
+    fc.reduce_point_count = r->s.reduce_point_count ? 1 : 0;
+    fc.cull_small = r->s.cull_small_gaussians ? 1 : 0;
+    fc.enable_occlusion = r->s.enable_occlusion_culling ? 1 : 0;
+    fc.enable_hier = (r->s.enable_hierarchical_culling && !r->s.fully_disable_hierarchical_culling) ? 1 : 0;
+    fc.width = r->s.width;
+    fc.height = r->s.height;
+    return fc;
+}
+
+BlockView block_view(gps_renderer* r) {
+    BlockView b{};
+    b.nodes = r->scene->block_nodes.get();
+    b.culled = r->culled.get();
+    b.node_count = r->scene->block_count;
+    b.words = (b.node_count + 31) / 32;
+    b.per_block = r->scene->per_block;
+    return b;
+}
+
+void count_launch(gps_renderer* r, int stage, uint64_t n = 1) {
+    r->frame_launches += n;
+    r->timer.launches[stage] += n;
+}
+
+void render_pass(gps_renderer* r, const FrameConst& fc, int frame, bool first, cudaStream_t st) {
+    const int frame_seed = 4 * frame + (first ? 0 : 2);
+    BlockView blocks = block_view(r);
+    if (fc.enable_hier && blocks.node_count) {
+        r->timer.mark(kStCull, st);
+        launch_block_cull(blocks, fc, r->hiz, st);
+        count_launch(r, kStCull);
+    }
+    r->timer.mark(kStPreprocess, st);
+    PreprocessArgs pa{};
+    pa.fc = fc;
+    pa.frame_seed = frame_seed;
+    pa.only_previously_occluded = first ? 0 : 1;
+    pa.n = r->n;
+    pa.counts = r->counts.get();
+    pa.mask_cur = r->mask[r->iteration % 2].get();
+    pa.mask_prev = r->mask[(r->iteration + 1) % 2].get();
+    pa.records = r->records.get();
+    pa.hiz = r->hiz;
+    pa.blocks = blocks;
+    if (r->scene->format == GPS_SCENE_FP32) {
+        SceneFP32 s{r->scene->pos_op.get(), r->scene->rot.get(), r->scene->scale.get(), r->scene->sh.get(), r->n};
+        launch_preprocess_fp32(pa, s, st);
+    } else {
+        SceneCompressed s{};
+        s.geom = r->scene->geom.get();
+        s.opac = r->scene->opac.get();
+        s.sh_dc = r->scene->sh_dc.get();
+        s.sh_ac = r->scene->sh_ac.get();
+        s.bounds = r->scene->bounds;
+        s.n = r->n;
+        launch_preprocess_compressed(pa, s, st);
+    }
+    count_launch(r, kStPreprocess);
+    r->timer.mark(kStScan, st);
+    PassCounters* pc = r->counters.get() + (first ? 0 : 1);
+    ScanArgs sa{};
+    sa.counts = r->counts.get();
+    sa.mask = pa.mask_cur;
+    sa.n = r->n;
+    sa.max_points = (uint32_t)std::max(0, r->s.max_number_of_points);
+    sa.tile_points = 256;
+    sa.surv_gid = r->surv_gid.get();
+    sa.surv_start = r->surv_start.get();
+    sa.tile_first_rank = r->tile_first_rank.get();
+    sa.tile_state = r->tile_state.get();
+    sa.tile_ticket = r->ticket.get();
+    sa.counters = pc;
+    launch_scan(sa, r->scan_tiles, st);
+    count_launch(r, kStScan, r->scan_tiles ? 1 : 0);
+    r->timer.mark(kStSplat, st);
+    SplatArgs sp{};
+    sp.fc = fc;
+    sp.frame_seed = frame_seed + 1;
+    sp.records = r->records.get();
+    sp.surv_gid = r->surv_gid.get();
+    sp.surv_start = r->surv_start.get();
+    sp.tile_first_rank = r->tile_first_rank.get();
+    sp.counters = pc;
+    sp.buffer = r->buffer.get();
+    sp.n = r->n;
+    launch_splat(sp, r->splat_grid, 256, st);
+    count_launch(r, kStSplat);
+    r->iteration++;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------------
+// C-ABI
+// ---------------------------------------------------------------------------------
+extern "C" {
+
+int32_t gps_abi_version(void) { return GPS_B200_ABI_VERSION; }
+const char* gps_last_error(void) { return last_error(); }
+
+void gps_settings_default(gps_settings* s) {
+    if (!s) return;
+    std::memset(s, 0, sizeof(*s));
+    s->width = 1920;
+    s->height = 1080;
+    s->supersampling_factor = 2;
+    s->samples_per_pixel = 1;
+    s->max_number_of_points = 250000000;
+    s->fovy = 45.0f;
+    s->near_view_plane = 0.2f;
+    s->far_view_plane = 10000.0f;
+    s->enable_hierarchical_culling = 1;
+    s->fully_disable_hierarchical_culling = 0;
+    s->enable_occlusion_culling = 1;
+    s->occlusion_culling_min_reduce_count = 0;
+    s->cull_small_gaussians = 0;
+    s->use_unbiased_2d_splatting = 1;
+    s->reduce_point_count = 1;
+    s->accumulation_mode = GPS_ACCUM_PROGRESSIVE;
+    s->sort_morton_order = 0;
+}
+
+gps_status gps_settings_parse_args(int32_t argc, const char* const* argv, gps_settings* s, char* model_path,
+                                   size_t model_cap, char* camera_path, size_t camera_cap) {
+    if (!s || (argc > 0 && !argv)) return fail(GPS_ERR_INVALID_ARGUMENT, "null argument");
+    auto need = [&](int i, int k) { return i + k < argc; };
+    auto put = [](char* dst, size_t cap, const char* v) {
+        if (dst && cap) {
+            std::strncpy(dst, v, cap - 1);
+            dst[cap - 1] = 0;
+        }
+    };
+    try {
+        for (int i = 1; i < argc; ++i) {
+            std::string a = argv[i];
+            if (a == "--background" && need(i, 3)) {
+                for (int k = 0; k < 3; ++k) s->background[k] = std::stof(argv[++i]);
+            } else if (a == "--fovy" && need(i, 1)) {
+                s->fovy = std::stof(argv[++i]);
+            } else if ((a == "--near-view-plane" || a == "--near_view_plane") && need(i, 1)) {
+                s->near_view_plane = std::stof(argv[++i]);
+            } else if ((a == "--far-view-plane" || a == "--far_view_plane") && need(i, 1)) {
+                s->far_view_plane = std::stof(argv[++i]);
+            } else if ((a == "--samples-per-pixel" || a == "--samples_per_pixel") && need(i, 1)) {
+                s->samples_per_pixel = std::stoi(argv[++i]);
+            } else if ((a == "--max-number-of-points" || a == "--max_number_of_points") && need(i, 1)) {
+                s->max_number_of_points = std::stoi(argv[++i]);
+            } else if ((a == "--supersampling-factor" || a == "--supersampling_factor") && need(i, 1)) {
+                s->supersampling_factor = std::stoi(argv[++i]);
+            } else if (a == "--resolution" && need(i, 2)) {
+                s->width = (int)std::stof(argv[++i]);
+                s->height = (int)std::stof(argv[++i]);
+            } else if ((a == "--set-target-width" || a == "--set_target_width") && need(i, 1)) {
+                s->width = std::stoi(argv[++i]);
+            } else if (a == "--cull-small") {
+                s->cull_small_gaussians = 1;
+            } else if (a == "--one_point_per_thread" || a == "--one-point-per-thread") {
+                s->reduce_point_count = 0;
+            } else if (a == "--disable_hierarchical_culling" || a == "--disable-hierarchical-culling") {
+                s->enable_hierarchical_culling = 0;
+            } else if (a == "--disable_occlusion_culling" || a == "--disable-occlusion-culling") {
+                s->enable_occlusion_culling = 0;
+            } else if (a == "--sort_morton_order" || a == "--sort-morton-order") {
+                s->sort_morton_order = 1;
+            } else if (a == "--taa") {
+                s->accumulation_mode = GPS_ACCUM_TAA;
+            } else if ((a == "--cameras-path" || a == "--camera-path") && need(i, 1)) {
+                put(camera_path, camera_cap, argv[++i]);
+            } else if (a == "--model-path" && need(i, 1)) {
+                put(model_path, model_cap, argv[++i]);
+            }
+            // other viewer flags (--disable-gui, --run-tests, ...) are accepted and ignored,
+            // as the reference ignores unknown ones (parse_args.cuh:120-122)
+        }
+    } catch (const std::exception& e) {
+        return fail(GPS_ERR_INVALID_ARGUMENT, std::string("bad numeric argument: ") + e.what());
+    }
+    return GPS_OK;
+}
+
+static gps_status scene_create(std::vector<CpuGaussian>& g, int32_t format, bool presorted, gps_scene** out) {
+    if (format != GPS_SCENE_FP32 && format != GPS_SCENE_COMPRESSED) return fail(GPS_ERR_INVALID_ARGUMENT, "unknown scene format");
+    if (g.size() >= (1ull << 30)) return fail(GPS_ERR_SIZE, "scenes are limited to 2^30 Gaussians");
+    auto s = std::make_unique<gps_scene>();
+    s->format = format;
+    s->presorted = presorted;
+    try {
+        scene_upload(s.get(), g.data(), g.size());
+    } catch (const CudaError& e) {
+        return fail(std::string(e.what()).find("cudaMalloc") != std::string::npos ? GPS_ERR_OUT_OF_MEMORY : GPS_ERR_CUDA, e.what());
+    }
+    *out = s.release();
+    return GPS_OK;
+}
+
+gps_status gps_scene_load_ply(const char* path, int32_t format, int32_t sort_morton_order, gps_scene** out,
+                              int32_t* presorted_out) {
+    if (!path || !out) return fail(GPS_ERR_INVALID_ARGUMENT, "null argument");
+    *out = nullptr;
+    std::string resolved;
+    int rc = resolve_model_path(path, resolved);
+    if (rc) return (gps_status)rc;
+    std::vector<CpuGaussian> g;
+    std::vector<std::string> comments;
+    rc = ply_read(resolved, g, comments);
+    if (rc) return (gps_status)rc;
+    bool presorted = has_bvh_sorted_comment(comments);
+    if (sort_morton_order && !presorted) morton_sort(g);
+    if (presorted_out) *presorted_out = presorted ? 1 : 0;
+    return scene_create(g, format, presorted, out);
+}
+
+gps_status gps_scene_from_host(const float* gaussians, uint64_t count, int32_t format, int32_t presorted,
+                               gps_scene** out) {
+    if (!out || (!gaussians && count)) return fail(GPS_ERR_INVALID_ARGUMENT, "null argument");
+    *out = nullptr;
+    std::vector<CpuGaussian> g(count);
+    if (count) std::memcpy(g.data(), gaussians, count * sizeof(CpuGaussian));
+    return scene_create(g, format, presorted != 0, out);
+}
+
+uint64_t gps_scene_count(const gps_scene* scene) { return scene ? scene->n : 0; }
+int32_t gps_scene_format_of(const gps_scene* scene) { return scene ? scene->format : -1; }
+void gps_scene_free(gps_scene* scene) { delete scene; }
+
+gps_status gps_ply_write(const char* path, const float* gaussians, uint64_t count, const char* comments) {
+    if (!path || (!gaussians && count)) return fail(GPS_ERR_INVALID_ARGUMENT, "null argument");
+    std::vector<std::string> cs;
+    if (comments) {
+        std::string c = comments, cur;
+        for (char ch : c) {
+            if (ch == '\n') {
+                if (!cur.empty()) cs.push_back(cur);
+                cur.clear();
+            } else cur += ch;
+        }
+        if (!cur.empty()) cs.push_back(cur);
+    }
+    int rc = ply_write(path, reinterpret_cast<const CpuGaussian*>(gaussians), count, cs);
+    return (gps_status)rc;
+}
+
+gps_status gps_ply_read(const char* path, float* out, uint64_t capacity, uint64_t* count, int32_t* presorted) {
+    if (!path || !count) return fail(GPS_ERR_INVALID_ARGUMENT, "null argument");
+    std::string resolved;
+    int rc = resolve_model_path(path, resolved);
+    if (rc) return (gps_status)rc;
+    std::vector<CpuGaussian> g;
+    std::vector<std::string> comments;
+    rc = ply_read(resolved, g, comments);
+    if (rc) return (gps_status)rc;
+    *count = g.size();
+    if (presorted) *presorted = has_bvh_sorted_comment(comments) ? 1 : 0;
+    if (out) {
+        if (capacity < g.size()) return fail(GPS_ERR_SIZE, "output capacity too small");
+        std::memcpy(out, g.data(), g.size() * sizeof(CpuGaussian));
+    }
+    return GPS_OK;
+}
+
+gps_status gps_renderer_create(gps_scene* scene, const gps_settings* settings, gps_renderer** out) {
+    if (!scene || !settings || !out) return fail(GPS_ERR_INVALID_ARGUMENT, "null argument");
+    *out = nullptr;
+    const gps_settings& s = *settings;
+    if (s.width <= 0 || s.height <= 0 || s.supersampling_factor <= 0 || s.samples_per_pixel <= 0)
+        return fail(GPS_ERR_INVALID_ARGUMENT, "resolution, supersampling factor and samples per pixel must be positive");
+    if (!(s.far_view_plane > s.near_view_plane) || !(s.fovy > 0.0f))
+        return fail(GPS_ERR_INVALID_ARGUMENT, "need far > near and fovy > 0");
+    const uint64_t up_w = (uint64_t)s.width * s.supersampling_factor, up_h = (uint64_t)s.height * s.supersampling_factor;
+    if (up_w > 65504 || up_h > 65504) return fail(GPS_ERR_SIZE, "supersampled resolution above 65504 pixels per axis");
+    const uint64_t entries = splat_buffer_entries((int)up_w, (int)up_h, s.samples_per_pixel);
+    if (entries >= (1ull << 31)) return fail(GPS_ERR_SIZE, "splat buffer above 2^31 entries");
+    auto r = std::make_unique<gps_renderer>();
+    r->scene = scene;
+    r->s = s;
+    r->up_w = (int)up_w;
+    r->up_h = (int)up_h;
+    r->entries = entries;
+    r->n = (uint32_t)scene->n;
+    r->scan_tiles = scan_tile_count(r->n);
+    r->n_pad = r->scan_tiles * 4096;
+    try {
+        r->buffer.reset(dev_alloc<uint64_t>(entries));
+        r->counts.reset(dev_alloc<uint32_t>(std::max<uint32_t>(r->n_pad, 16)));
+        GPS_CUDA(cudaMemset(r->counts.get(), 0, sizeof(uint32_t) * std::max<uint32_t>(r->n_pad, 16)));
+        const uint32_t words = (r->n + 31) / 32;
+        for (int i = 0; i < 2; ++i) {
+            r->mask[i].reset(dev_alloc<uint32_t>(words + 1));
+            GPS_CUDA(cudaMemset(r->mask[i].get(), 0, sizeof(uint32_t) * (words + 1)));
+        }
+        r->records.reset(dev_alloc<SplatRecord>(std::max<uint32_t>(r->n, 1)));
+        r->surv_gid.reset(dev_alloc<uint32_t>(std::max<uint32_t>(r->n, 1)));
+        r->surv_start.reset(dev_alloc<uint32_t>(std::max<uint32_t>(r->n, 1)));
+        const uint64_t max_pts = (uint64_t)std::max(0, s.max_number_of_points);
+        r->tile_first_rank.reset(dev_alloc<uint32_t>(max_pts / 256 + 2));
+        r->tile_state.reset(dev_alloc<unsigned long long>(std::max<uint32_t>(r->scan_tiles, 1)));
+        r->ticket.reset(dev_alloc<uint32_t>(1));
+        r->counters.reset(dev_alloc<PassCounters>(2));
+        GPS_CUDA(cudaMemset(r->counters.get(), 0, sizeof(PassCounters) * 2));
+        const uint32_t bwords = (scene->block_count + 31) / 32;
+        r->culled.reset(dev_alloc<uint32_t>(bwords + 1));
+        GPS_CUDA(cudaMemset(r->culled.get(), 0, sizeof(uint32_t) * (bwords + 1)));
+        hiz_layout(r->hiz, s.width, s.height);
+        r->mip.reset(dev_alloc<float>(r->hiz.mip_size));
+        r->hiz.mip = r->mip.get();
+        // the reference leaves its Hi-Z uninitialised before the first frame; +inf here
+        // means "nothing occluded" for frame 1
+        fill_f32<<<148 * 4, 256>>>(r->mip.get(), r->hiz.mip_size, INFINITY);
+        GPS_CUDA(cudaGetLastError());
+        GPS_CUDA(cudaMallocHost(&r->host_counters, sizeof(PassCounters) * 2));
+        std::memset(r->host_counters, 0, sizeof(PassCounters) * 2);
+        GPS_CUDA(cudaEventCreateWithFlags(&r->done, cudaEventDisableTiming));
+        r->splat_grid = splat_grid_size(256);
+        GPS_CUDA(cudaDeviceSynchronize());
+    } catch (const CudaError& e) {
+        return fail(std::string(e.what()).find("cudaMalloc") != std::string::npos ? GPS_ERR_OUT_OF_MEMORY : GPS_ERR_CUDA, e.what());
+    }
+    *out = r.release();
+    return GPS_OK;
+}
+
+void gps_renderer_free(gps_renderer* r) {
+    if (r) cudaDeviceSynchronize();
+    delete r;
+}
+
+gps_status gps_render_frame(gps_renderer* r, const gps_camera* cam, float* d_image, float* d_depth, void* stream) {
+    if (!r || !cam || !d_image || !d_depth) return fail(GPS_ERR_INVALID_ARGUMENT, "null argument");
+    cudaStream_t st = as_stream(stream);
+    const FrameConst fc = make_frame_const(r, cam);
+    const uint64_t bg = 0xFFFFFFF000000000ull |
+                        rgb_to_36bits(make_v3(r->s.background[0], r->s.background[1], r->s.background[2]));
+    r->frame_launches = 0;
+    r->timer.mark(kStClear, st);
+    launch_clear(r->buffer.get(), r->entries, bg, st);
+    count_launch(r, kStClear);
+    if (r->n > 0) render_pass(r, fc, cam->frame, true, st);
+    ResolveArgs ra{};
+    ra.buffer = r->buffer.get();
+    ra.color = d_image;
+    ra.depth = d_depth;
+    ra.width = r->s.width;
+    ra.height = r->s.height;
+    ra.num_passes = r->s.samples_per_pixel;
+    ra.ss = r->s.supersampling_factor;
+    ra.entries = r->entries;
+    ra.near_plane = r->s.near_view_plane;
+    ra.far_plane = r->s.far_view_plane;
+    ra.initial_value = bg;
+    r->second_pass_last = false;
+    if (r->s.enable_occlusion_culling) {
+        r->timer.mark(kStResolve, st);
+        launch_resolve(ra, true, st);
+        count_launch(r, kStResolve);
+        r->timer.mark(kStHiz, st);
+        launch_hiz_build(r->hiz, d_depth, r->s.occlusion_culling_min_reduce_count, st);
+        count_launch(r, kStHiz, (uint64_t)r->hiz.levels);
+        if (r->n > 0) {
+            render_pass(r, fc, cam->frame, false, st);
+            r->second_pass_last = true;
+        }
+    } else {
+        cudaMemsetAsync(r->counters.get() + 1, 0, sizeof(PassCounters), st);
+    }
+    r->timer.mark(kStResolve, st);
+    launch_resolve(ra, false, st);
+    count_launch(r, kStResolve);
+    if (r->s.enable_occlusion_culling) {
+        r->timer.mark(kStHiz, st);
+        launch_hiz_build(r->hiz, d_depth, r->s.occlusion_culling_min_reduce_count, st);
+        count_launch(r, kStHiz, (uint64_t)r->hiz.levels);
+    }
+    r->timer.mark(-1, st);
+    cudaMemcpyAsync(r->host_counters, r->counters.get(), sizeof(PassCounters) * 2, cudaMemcpyDeviceToHost, st);
+    cudaEventRecord(r->done, st);
+    r->have_frame = true;
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return fail(GPS_ERR_CUDA, std::string("frame launch failed: ") + cudaGetErrorString(e));
+    return GPS_OK;
+}
+
+gps_status gps_renderer_stats(gps_renderer* r, gps_stats* out) {
+    if (!r || !out) return fail(GPS_ERR_INVALID_ARGUMENT, "null argument");
+    std::memset(out, 0, sizeof(*out));
+    if (!r->have_frame) return GPS_OK;
+    cudaError_t e = cudaEventSynchronize(r->done);
+    if (e != cudaSuccess) return fail(GPS_ERR_CUDA, std::string("frame failed: ") + cudaGetErrorString(e));
+    const PassCounters* c = r->host_counters;
+    out->num_points_one = (int32_t)c[0].points;
+    out->num_points_two = (int32_t)c[1].points;
+    out->num_gaussians_one = (int32_t)r->n;
+    out->num_gaussians_two = r->s.enable_occlusion_culling ? (int32_t)r->n : 0;
+    out->survivors_one = (int32_t)c[0].survivors;
+    out->survivors_two = (int32_t)c[1].survivors;
+    out->total_points_one = c[0].total_points;
+    out->total_points_two = c[1].total_points;
+    out->truncated = (int32_t)(c[0].truncated | c[1].truncated);
+    out->device_timeouts = (int32_t)(c[0].scan_timeouts + c[1].scan_timeouts);
+    out->kernel_launches = (int32_t)r->frame_launches;
+    if (out->device_timeouts) return fail(GPS_ERR_DEVICE_TIMEOUT, "a device-side look-back wait gave up");
+    return GPS_OK;
+}
+
+gps_status gps_renderer_enable_timing(gps_renderer* r, int32_t enable) {
+    if (!r) return fail(GPS_ERR_INVALID_ARGUMENT, "null argument");
+    StageTimer& t = r->timer;
+    if (enable && t.pool.empty()) {
+        t.pool.resize(4096);
+        t.stage.assign(4096, -1);
+        for (auto& e : t.pool) {
+            cudaError_t err = cudaEventCreate(&e);
+            if (err != cudaSuccess) return fail(GPS_ERR_CUDA, cudaGetErrorString(err));
+        }
+    }
+    t.drain();
+    t.on = enable != 0;
+    return GPS_OK;
+}
+
+gps_status gps_renderer_stage_times(gps_renderer* r, float* out_ms, uint64_t* out_launches, int32_t reset) {
+    if (!r || !out_ms) return fail(GPS_ERR_INVALID_ARGUMENT, "null argument");
+    r->timer.drain();
+    for (int i = 0; i < kStCount; ++i) {
+        out_ms[i] = (float)r->timer.total_ms[i];
+        if (out_launches) out_launches[i] = r->timer.launches[i];
+    }
+    if (reset) {
+        for (int i = 0; i < kStCount; ++i) {
+            r->timer.total_ms[i] = 0.0;
+            r->timer.launches[i] = 0;
+        }
+    }
+    return GPS_OK;
+}
+
+gps_status gps_renderer_splat_buffer(gps_renderer* r, const uint64_t** d_buffer, uint64_t* entries) {
+    if (!r || !d_buffer || !entries) return fail(GPS_ERR_INVALID_ARGUMENT, "null argument");
+    *d_buffer = r->buffer.get();
+    *entries = r->entries;
+    return GPS_OK;
+}
+
+gps_status gps_renderer_derived(gps_renderer* r, const gps_camera* cam, float* out36) {
+    if (!r || !cam || !out36) return fail(GPS_ERR_INVALID_ARGUMENT, "null argument");
+    FrameConst fc = make_frame_const(r, cam);
+    mat4_to(fc.vp, out36);
+    mat4_to(fc.cam, out36 + 16);
+    out36[32] = fc.tan_fov.x;
+    out36[33] = fc.tan_fov.y;
+    out36[34] = fc.focal.x;
+    out36[35] = fc.focal.y;
+    return GPS_OK;
+}
+
+gps_status gps_renderer_debug_view(gps_renderer* r, gps_debug_view* out) {
+    if (!r || !out) return fail(GPS_ERR_INVALID_ARGUMENT, "null argument");
+    std::memset(out, 0, sizeof(*out));
+    if (r->have_frame) {
+        cudaError_t e = cudaEventSynchronize(r->done);
+        if (e != cudaSuccess) return fail(GPS_ERR_CUDA, cudaGetErrorString(e));
+    }
+    out->counts = r->counts.get();
+    // after a pass the iteration counter has advanced: the last pass wrote mask[(it-1)%2]
+    out->mask_last = r->mask[(r->iteration + 1) % 2].get();
+    out->mask_other = r->mask[r->iteration % 2].get();
+    out->surv_gid = r->surv_gid.get();
+    out->surv_start = r->surv_start.get();
+    const PassCounters& c = r->host_counters[r->second_pass_last ? 1 : 0];
+    out->survivors = c.survivors;
+    out->points = c.points;
+    out->records = reinterpret_cast<const float*>(r->records.get());
+    out->hiz = r->mip.get();
+    out->hiz_size = r->hiz.mip_size;
+    out->block_culled = r->culled.get();
+    out->block_words = (r->scene->block_count + 31) / 32;
+    out->block_nodes = reinterpret_cast<const float*>(r->scene->block_nodes.get());
+    out->block_count = r->scene->block_count;
+    out->per_block = r->scene->per_block;
+    return GPS_OK;
+}
+
+gps_status gps_post_taa(uint8_t* d_image_u8, float* d_out_color, const float* d_cur_color, const float* d_prev_color,
+                        const float* d_cur_depth, const float* d_prev_depth, const float* reproj16, float blend,
+                        int32_t width, int32_t height, int32_t frame_number, void* stream) {
+    if (!d_image_u8 || !d_out_color || !d_cur_color || !d_prev_color || !d_cur_depth || !reproj16 || width <= 0 ||
+        height <= 0)
+        return fail(GPS_ERR_INVALID_ARGUMENT, "bad argument");
+    if (d_out_color == d_cur_color) return fail(GPS_ERR_INVALID_ARGUMENT, "d_out_color must not alias d_cur_color");
+    launch_taa(d_image_u8, d_out_color, d_cur_color, d_prev_color, d_cur_depth, d_prev_depth, mat4_from(reproj16), blend,
+               width, height, frame_number, as_stream(stream));
+    cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? GPS_OK : fail(GPS_ERR_CUDA, cudaGetErrorString(e));
+}
+
+gps_status gps_post_progressive(uint8_t* d_image_u8, float* d_cur_color, float* d_accum, int32_t width,
+                                int32_t height, int32_t frames, void* stream) {
+    if (!d_image_u8 || !d_cur_color || !d_accum || width <= 0 || height <= 0 || frames <= 0)
+        return fail(GPS_ERR_INVALID_ARGUMENT, "bad argument");
+    launch_progressive(d_image_u8, d_cur_color, d_accum, width, height, frames, as_stream(stream));
+    cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? GPS_OK : fail(GPS_ERR_CUDA, cudaGetErrorString(e));
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------------
+// headless frame loop (RenderServer::renderFrame, render_server.cu:86-157, without GL)
+// ---------------------------------------------------------------------------------
+struct gps_frame_loop {
+    gps_renderer* r = nullptr;
+    dptr<float> color[2], depth[2];
+    dptr<float> taa_out;  // TAA writes here, then swaps with the current colour slot
+    dptr<uint8_t> u8;
+    int progressive_frames = 0;
+    mat4 prev_vp{};
+};
+
+extern "C" {
+
+gps_status gps_frame_loop_create(gps_renderer* r, gps_frame_loop** out) {
+    if (!r || !out) return fail(GPS_ERR_INVALID_ARGUMENT, "null argument");
+    auto l = std::make_unique<gps_frame_loop>();
+    l->r = r;
+    const size_t px = (size_t)r->s.width * r->s.height;
+    try {
+        for (int i = 0; i < 2; ++i) {
+            l->color[i].reset(dev_alloc<float>(px * 3));
+            l->depth[i].reset(dev_alloc<float>(px));
+            GPS_CUDA(cudaMemset(l->color[i].get(), 0, px * 3 * sizeof(float)));
+            GPS_CUDA(cudaMemset(l->depth[i].get(), 0, px * sizeof(float)));
+        }
+        l->u8.reset(dev_alloc<uint8_t>(px * 3));
+        GPS_CUDA(cudaMemset(l->u8.get(), 0, px * 3));
+        l->taa_out.reset(dev_alloc<float>(px * 3));
+    } catch (const CudaError& e) {
+        return fail(GPS_ERR_OUT_OF_MEMORY, e.what());
+    }
+    for (int c = 0; c < 4; ++c) l->prev_vp.c[c] = make_v4(c == 0, c == 1, c == 2, c == 3);
+    *out = l.release();
+    return GPS_OK;
+}
+
+void gps_frame_loop_free(gps_frame_loop* l) { delete l; }
+
+gps_status gps_frame_loop_step(gps_frame_loop* l, const gps_camera* cam, void* stream) {
+    if (!l || !cam) return fail(GPS_ERR_INVALID_ARGUMENT, "null argument");
+    gps_renderer* r = l->r;
+    const int a = cam->frame % 2, b = 1 - a;
+    gps_status st = gps_render_frame(r, cam, l->color[a].get(), l->depth[b].get(), stream);
+    if (st != GPS_OK) return st;
+    const int w = r->s.width, h = r->s.height;
+    mat4 view = mat4_from(cam->view), proj = mat4_from(cam->proj);
+    r->timer.mark(kStPost, as_stream(stream));
+    r->frame_launches += 1;
+    r->timer.launches[kStPost] += 1;
+    if (r->s.accumulation_mode == GPS_ACCUM_TAA) {
+        l->progressive_frames++;
+        mat4 model = affine_inverse(view);
+        mat4 delta = mat4_mul(mat4_mul(l->prev_vp, model), inverse4(proj));
+        launch_taa(l->u8.get(), l->taa_out.get(), l->color[a].get(), l->color[b].get(), l->depth[a].get(),
+                   l->depth[b].get(), delta, 0.9f, w, h, l->progressive_frames, as_stream(stream));
+        std::swap(l->color[a], l->taa_out);
+    } else {
+        if (cam->camera_moved || r->s.accumulation_mode == GPS_ACCUM_NONE) l->progressive_frames = 1;
+        else l->progressive_frames++;
+        launch_progressive(l->u8.get(), l->color[a].get(), l->color[b].get(), w, h, l->progressive_frames,
+                           as_stream(stream));
+    }
+    r->timer.mark(-1, as_stream(stream));
+    l->prev_vp = mat4_mul(proj, view);
+    cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? GPS_OK : fail(GPS_ERR_CUDA, cudaGetErrorString(e));
+}
+
+gps_status gps_frame_loop_read(gps_frame_loop* l, uint8_t* host_rgb, void* stream) {
+    if (!l || !host_rgb) return fail(GPS_ERR_INVALID_ARGUMENT, "null argument");
+    const size_t bytes = (size_t)l->r->s.width * l->r->s.height * 3;
+    cudaError_t e = cudaMemcpyAsync(host_rgb, l->u8.get(), bytes, cudaMemcpyDeviceToHost, as_stream(stream));
+    if (e == cudaSuccess) e = cudaStreamSynchronize(as_stream(stream));
+    return e == cudaSuccess ? GPS_OK : fail(GPS_ERR_CUDA, cudaGetErrorString(e));
+}
+
+gps_status gps_frame_loop_buffers(gps_frame_loop* l, int32_t slot, const uint8_t** d_u8, const float** d_color,
+                                  const float** d_depth) {
+    if (!l || slot < 0 || slot > 1) return fail(GPS_ERR_INVALID_ARGUMENT, "bad argument");
+    if (d_u8) *d_u8 = l->u8.get();
+    if (d_color) *d_color = l->color[slot].get();
+    if (d_depth) *d_depth = l->depth[slot].get();
+    return GPS_OK;
+}
+
+// ---- cameras --------------------------------------------------------------------------
+}  // extern "C"
+
+struct gps_camera_path {
+    std::vector<CameraState> states;
+};
+
+extern "C" {
+
+gps_status gps_camera_path_load(const char* json_path, gps_camera_path** out) {
+    if (!json_path || !out) return fail(GPS_ERR_INVALID_ARGUMENT, "null argument");
+    *out = nullptr;
+    auto p = std::make_unique<gps_camera_path>();
+    int rc = load_cameras(json_path, p->states);
+    if (rc) return (gps_status)rc;
+    *out = p.release();
+    return GPS_OK;
+}
+
+int32_t gps_camera_path_count(const gps_camera_path* p) { return p ? (int32_t)p->states.size() : 0; }
+
+gps_status gps_camera_path_get(const gps_camera_path* p, int32_t index, gps_camera_state* out) {
+    if (!p || !out) return fail(GPS_ERR_INVALID_ARGUMENT, "null argument");
+    if (index < 0 || index >= (int32_t)p->states.size()) return fail(GPS_ERR_INVALID_ARGUMENT, "camera index out of range");
+    const CameraState& c = p->states[index];
+    std::memset(out, 0, sizeof(*out));
+    out->id = c.id;
+    out->width = c.width;
+    out->height = c.height;
+    for (int i = 0; i < 3; ++i) out->position[i] = c.position[i];
+    for (int i = 0; i < 9; ++i) out->rotation[i] = c.rotation[i];
+    out->fx = c.fx;
+    out->fy = c.fy;
+    std::strncpy(out->img_name, c.img_name.c_str(), sizeof(out->img_name) - 1);
+    return GPS_OK;
+}
+
+void gps_camera_path_free(gps_camera_path* p) { delete p; }
+
+static void fill_camera(const CameraMatrices& m, int32_t frame, gps_camera* cam) {
+    std::memset(cam, 0, sizeof(*cam));
+    mat4_to(m.view, cam->view);
+    mat4_to(m.proj, cam->proj);
+    cam->position[0] = m.position.x;
+    cam->position[1] = m.position.y;
+    cam->position[2] = m.position.z;
+    for (int i = 0; i < 6; ++i) {
+        cam->frustum_planes[4 * i] = m.planes[i].x;
+        cam->frustum_planes[4 * i + 1] = m.planes[i].y;
+        cam->frustum_planes[4 * i + 2] = m.planes[i].z;
+        cam->frustum_planes[4 * i + 3] = m.planes[i].w;
+    }
+    cam->frame = frame;
+}
+
+gps_status gps_camera_from_state(const gps_camera_state* state, gps_settings* settings, int32_t override_camera_settings,
+                                 int32_t* can_override_resolution, int32_t frame, gps_camera* cam) {
+    if (!state || !settings || !cam) return fail(GPS_ERR_INVALID_ARGUMENT, "null argument");
+    // basis = transpose(rotation) where rotation's glm columns are the JSON rows
+    mat3 rot_glm;
+    for (int c = 0; c < 3; ++c) rot_glm.c[c] = make_v3(state->rotation[3 * c], state->rotation[3 * c + 1], state->rotation[3 * c + 2]);
+    mat3 basis = transpose(rot_glm);
+    float q[4];
+    quat_from_basis(basis, q);
+    if (!override_camera_settings) {
+        int can = can_override_resolution ? *can_override_resolution : 1;
+        if (can) {
+            float aspect_yx = (float)state->height / (float)state->width;
+            float rx = roundf((float)settings->width);
+            float ry = roundf((float)settings->width * aspect_yx);
+            settings->width = (int)rx;
+            settings->height = (int)ry;
+            if (can_override_resolution) *can_override_resolution = 0;
+        }
+        settings->fovy = focal_to_fov_deg(state->fy, state->height);
+    }
+    float aspect = (float)settings->width / (float)settings->height;
+    CameraMatrices m = camera_matrices(make_v3(state->position[0], state->position[1], state->position[2]), q,
+                                       settings->fovy, aspect, settings->near_view_plane, settings->far_view_plane);
+    fill_camera(m, frame, cam);
+    return GPS_OK;
+}
+
+gps_status gps_camera_from_pose(const float position[3], const float basis_cols[9], const gps_settings* settings,
+                                int32_t frame, gps_camera* cam) {
+    if (!position || !basis_cols || !settings || !cam) return fail(GPS_ERR_INVALID_ARGUMENT, "null argument");
+    mat3 basis;
+    for (int c = 0; c < 3; ++c) basis.c[c] = make_v3(basis_cols[3 * c], basis_cols[3 * c + 1], basis_cols[3 * c + 2]);
+    float q[4];
+    quat_from_basis(basis, q);
+    float aspect = (float)settings->width / (float)settings->height;
+    CameraMatrices m = camera_matrices(make_v3(position[0], position[1], position[2]), q, settings->fovy, aspect,
+                                       settings->near_view_plane, settings->far_view_plane);
+    fill_camera(m, frame, cam);
+    return GPS_OK;
+}
+
+}  // extern "C"

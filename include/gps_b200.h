@@ -1,0 +1,229 @@
+/*
+ * gps_b200 — C-ABI of the B200-native Gaussian point-splatting frame path.
+ *
+ * Drop-in boundary for the reference's render pass (PeterZs/gaussian-point-splatting):
+ *   class RenderPass { virtual void render(glm::vec3* d_image, float* d_depth,
+ *                                          const RenderSettings&) = 0; }
+ *     src/core/rendering/render_pass.cuh:17-24, implemented by GaussianPointSplatting
+ *     (src/core/rendering/passes/gaussian_point_splatting.cuh:34-71, .cu:599-816).
+ * Plain pointers and sizes only; every call returns a gps_status and never traps or
+ * aborts.  Device pointers are CUDA global-memory addresses on the current device; the
+ * `stream` arguments are cudaStream_t values passed as void* (NULL = legacy stream).
+ */
+#ifndef GPS_B200_H
+#define GPS_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define GPS_B200_ABI_VERSION 1
+
+typedef enum gps_status {
+    GPS_OK = 0,
+    GPS_ERR_INVALID_ARGUMENT = 1,
+    GPS_ERR_IO = 2,             /* file missing / unreadable / short read */
+    GPS_ERR_FORMAT = 3,         /* malformed PLY header or camera JSON */
+    GPS_ERR_CUDA = 4,           /* a CUDA runtime call failed */
+    GPS_ERR_OUT_OF_MEMORY = 5,
+    GPS_ERR_SIZE = 6,           /* request exceeds a supported size */
+    GPS_ERR_DEVICE_TIMEOUT = 7  /* a bounded device-side wait gave up */
+} gps_status;
+
+/* Scene storage formats on the device. */
+typedef enum gps_scene_format {
+    GPS_SCENE_FP32 = 0,        /* GPUGaussianSceneUncompressed (gaussian_types.cuh:548-646) */
+    GPS_SCENE_COMPRESSED = 1   /* GPUGaussianSceneCompressed, the reference's default build
+                                  (config.h:15, gaussian_types.cuh:421-541) */
+} gps_scene_format;
+
+typedef enum gps_accumulation {
+    GPS_ACCUM_PROGRESSIVE = 0, /* AccumulationMode::ProgressiveRendering */
+    GPS_ACCUM_TAA = 1,         /* AccumulationMode::TAA */
+    GPS_ACCUM_NONE = 2         /* AccumulationMode::None */
+} gps_accumulation;
+
+/*
+ * Render settings: the fields of RenderSettings (src/render_settings.cuh:36-103) that the
+ * frame path reads, with the same defaults (gps_settings_default).
+ */
+typedef struct gps_settings {
+    int32_t width, height;                      /* resolution (1920 x 1080) */
+    int32_t supersampling_factor;               /* 2 */
+    int32_t samples_per_pixel;                  /* render_pass_count, 1 */
+    int32_t max_number_of_points;               /* 250000000 */
+    float fovy;                                 /* degrees, 45 */
+    float near_view_plane, far_view_plane;      /* 0.2, 10000 */
+    int32_t enable_hierarchical_culling;        /* 1 */
+    int32_t fully_disable_hierarchical_culling; /* 0 */
+    int32_t enable_occlusion_culling;           /* 1 */
+    int32_t occlusion_culling_min_reduce_count; /* 0 */
+    int32_t cull_small_gaussians;               /* 0 */
+    int32_t use_unbiased_2d_splatting;          /* 1 */
+    int32_t reduce_point_count;                 /* 1: K = ss^2 points per thread; 0 = --one-point-per-thread */
+    float background[3];                        /* 0,0,0 */
+    int32_t accumulation_mode;                  /* gps_accumulation, progressive */
+    int32_t sort_morton_order;                  /* 0 */
+} gps_settings;
+
+/* One frame's camera: what RenderSettings carries per frame (render_settings.cuh:94-105). */
+typedef struct gps_camera {
+    float view[16];            /* cameraViewMatrix, column-major */
+    float proj[16];            /* cameraProjectionMatrix, column-major */
+    float position[3];         /* cameraPosition */
+    float frustum_planes[24];  /* 6 x (nx, ny, nz, d), left,right,bottom,top,near,far */
+    int32_t frame;             /* settings.frame (seeds, A/B buffers) */
+    int32_t camera_moved;      /* resets progressive accumulation */
+} gps_camera;
+
+/* One entry of a 3DGS cameras.json (src/utils/camera_loader.cuh:29-40). */
+typedef struct gps_camera_state {
+    int32_t id;
+    int32_t width, height;
+    float position[3];
+    float rotation[9];         /* rows as stored in the JSON (camera-to-world basis rows) */
+    float fx, fy;
+    char img_name[64];
+} gps_camera_state;
+
+/* Per-frame statistics (render_settings.cuh:23-34) plus device-side counters. */
+typedef struct gps_stats {
+    int32_t num_points_one, num_points_two;         /* P of pass 1 / pass 2 */
+    int32_t num_gaussians_one, num_gaussians_two;   /* Gaussians scanned per pass */
+    int32_t survivors_one, survivors_two;           /* Gaussians with >= 1 point per pass */
+    uint32_t total_points_one, total_points_two;    /* before the max_number_of_points clamp */
+    int32_t truncated;                              /* 1 if the point budget clipped a pass */
+    int32_t device_timeouts;                        /* bounded waits that gave up (0 normally) */
+    int32_t kernel_launches;                        /* kernels the last frame launched */
+} gps_stats;
+
+typedef struct gps_scene gps_scene;
+typedef struct gps_renderer gps_renderer;
+typedef struct gps_camera_path gps_camera_path;
+
+/* ---- version / errors -------------------------------------------------------------- */
+int32_t gps_abi_version(void);
+/* Last error message of the calling thread ("" if none). */
+const char* gps_last_error(void);
+
+/* ---- settings (render_settings.cuh:36-103, parse_args.cuh:21-127) ------------------- */
+void gps_settings_default(gps_settings* s);
+/* Parses the reference's CLI flags (--resolution W H, --supersampling-factor, ...).
+ * model_path/camera_path receive --model-path / --camera-path (may be NULL). */
+gps_status gps_settings_parse_args(int32_t argc, const char* const* argv, gps_settings* s,
+                                   char* model_path, size_t model_path_cap,
+                                   char* camera_path, size_t camera_path_cap);
+
+/* ---- scenes (gaussian_loader.cu:282-427, gaussian_types.cuh:442-503,568-608) ---------
+ * gps_scene_load_ply accepts a .ply file or a 3DGS output directory
+ * (point_cloud/<alphabetically last>/point_cloud.ply, render_settings.cuh:137-227).
+ * presorted_out (may be NULL) receives 1 if the file carries the bvh_sorted_order comment. */
+gps_status gps_scene_load_ply(const char* path, int32_t format, int32_t sort_morton_order,
+                              gps_scene** out, int32_t* presorted_out);
+/* Builds a scene from host Gaussians in the reference's CPUGaussian layout
+ * (gaussian_types.cuh:89-100): 59 floats each = mean[3], sh[48], opacity (activated),
+ * scale[3] (activated), rotation[4] (normalised, rot_0..rot_3). */
+gps_status gps_scene_from_host(const float* gaussians, uint64_t count, int32_t format,
+                               int32_t presorted, gps_scene** out);
+uint64_t gps_scene_count(const gps_scene* scene);
+int32_t gps_scene_format_of(const gps_scene* scene);
+void gps_scene_free(gps_scene* scene);
+/* Writes host Gaussians (CPUGaussian layout) as a 3DGS binary PLY with normals
+ * (gaussian_loader.cu:480-562); comments are '\n'-separated (may be NULL). */
+gps_status gps_ply_write(const char* path, const float* gaussians, uint64_t count, const char* comments);
+/* Reads a PLY into host memory in CPUGaussian layout (count first with out = NULL). */
+gps_status gps_ply_read(const char* path, float* out, uint64_t capacity, uint64_t* count, int32_t* presorted);
+
+/* ---- renderer = GaussianPointSplatting (gaussian_point_splatting.cu:599-816) -------- */
+gps_status gps_renderer_create(gps_scene* scene, const gps_settings* settings, gps_renderer** out);
+void gps_renderer_free(gps_renderer* r);
+/* RenderPass::render: writes the W x H float3 image and float NDC depth (caller-owned
+ * device buffers).  No host synchronisation and no allocation inside. */
+gps_status gps_render_frame(gps_renderer* r, const gps_camera* cam, float* d_image_rgb, float* d_depth,
+                            void* stream);
+/* Statistics of the last frame; waits for that frame's work on its stream. */
+gps_status gps_renderer_stats(gps_renderer* r, gps_stats* out);
+/* Per-stage GPU timing with CUDA events on the frame's stream (off by default).  Stages:
+ * 0 clear, 1 block cull, 2 preprocess, 3 scan, 4 splat, 5 resolve, 6 Hi-Z, 7 post-process;
+ * out_ms[8] receives the accumulated milliseconds, out_launches[8] (may be NULL) the kernel
+ * launches per stage, since enabling or the last reset. */
+gps_status gps_renderer_enable_timing(gps_renderer* r, int32_t enable);
+gps_status gps_renderer_stage_times(gps_renderer* r, float* out_ms, uint64_t* out_launches, int32_t reset);
+/* The current 64-bit splat buffer (depth28 << 36 | rgb36, Morton 64x64 tiles, spp innermost). */
+gps_status gps_renderer_splat_buffer(gps_renderer* r, const uint64_t** d_buffer, uint64_t* entries);
+/* Per-frame constants the renderer derived from the camera (gaussian_point_splatting.cu:605-615):
+ * out[0:16] view-projection, out[16:32] camera-to-world, out[32:34] tan_fov, out[34:36] focal. */
+gps_status gps_renderer_derived(gps_renderer* r, const gps_camera* cam, float* out36);
+/* Device views of the last pass's workload for parity checks: counts[N] (valid where the
+ * mask bit is set), mask words of the last two passes, survivors' Gaussian ids and first
+ * points, the Hi-Z chain, per-Gaussian colours (float3 inside 64-byte records), block mask. */
+typedef struct gps_debug_view {
+    const uint32_t* counts;
+    const uint32_t* mask_last;
+    const uint32_t* mask_other;
+    const uint32_t* surv_gid;
+    const uint32_t* surv_start;
+    uint32_t survivors;
+    uint32_t points;
+    const float* records;       /* 16 floats per Gaussian */
+    const float* hiz;
+    uint64_t hiz_size;
+    const uint32_t* block_culled;
+    uint32_t block_words;
+    const float* block_nodes;   /* 8 floats per node: min.xyz, begin bits, max.xyz, count bits */
+    uint32_t block_count;
+    uint32_t per_block;
+} gps_debug_view;
+gps_status gps_renderer_debug_view(gps_renderer* r, gps_debug_view* out);
+
+/* ---- RenderServer post-process (render_server.cu:122-157) ---------------------------- */
+/* temporalRender (post_processing_kernels.cuh:222-285): reprojects history through reproj
+ * (column-major), clamps it to the 3x3 neighbourhood of the current colour +-0.05, blends,
+ * writes the blended colour to d_out_color and u8 RGB to d_image_u8.  The reference blends in
+ * place, which races with the neighbourhood reads of adjacent threads; d_out_color must be a
+ * different buffer from d_cur_color, which makes the result deterministic. */
+gps_status gps_post_taa(uint8_t* d_image_u8, float* d_out_color, const float* d_cur_color,
+                        const float* d_prev_color, const float* d_cur_depth, const float* d_prev_depth,
+                        const float* reproj16, float blend, int32_t width, int32_t height,
+                        int32_t frame_number, void* stream);
+/* progressiveRender: cur += accum (frames > 1), accum = 0, u8 = round(clamp(cur*255/frames)). */
+gps_status gps_post_progressive(uint8_t* d_image_u8, float* d_cur_color, float* d_accum, int32_t width,
+                                int32_t height, int32_t frames, void* stream);
+
+/* ---- headless frame loop = RenderServer::renderFrame without GL -------------------- */
+/* Owns the colour/depth ping-pong buffers and the u8 output; reproduces the reference's
+ * buffer rotation (including its depth-slot order) and accumulation counter. */
+typedef struct gps_frame_loop gps_frame_loop;
+gps_status gps_frame_loop_create(gps_renderer* r, gps_frame_loop** out);
+void gps_frame_loop_free(gps_frame_loop* l);
+/* Renders one frame and post-processes it; d_image_u8 may be NULL (internal buffer). */
+gps_status gps_frame_loop_step(gps_frame_loop* l, const gps_camera* cam, void* stream);
+/* Copies the last u8 RGB frame (W*H*3 bytes) to host memory. */
+gps_status gps_frame_loop_read(gps_frame_loop* l, uint8_t* host_rgb, void* stream);
+/* Device buffers of ping-pong slot `slot` (0 or 1): frame f renders its colour into slot
+ * f % 2 and its depth into slot 1 - f % 2 (render_server.cu:87-92). */
+gps_status gps_frame_loop_buffers(gps_frame_loop* l, int32_t slot, const uint8_t** d_u8, const float** d_color,
+                                  const float** d_depth);
+
+/* ---- cameras (camera_loader.cu:62-150, main.cu:141-157, camera.cpp:88-156) ---------- */
+gps_status gps_camera_path_load(const char* json_path, gps_camera_path** out);
+int32_t gps_camera_path_count(const gps_camera_path* p);
+gps_status gps_camera_path_get(const gps_camera_path* p, int32_t index, gps_camera_state* out);
+void gps_camera_path_free(gps_camera_path* p);
+/* Applies fromCameraState's resolution/fovy override rules to *settings (when
+ * override_camera_settings == 0) and fills *cam with view, projection, planes, position. */
+gps_status gps_camera_from_state(const gps_camera_state* state, gps_settings* settings,
+                                 int32_t override_camera_settings, int32_t* can_override_resolution,
+                                 int32_t frame, gps_camera* cam);
+/* Builds view/projection/planes from a camera position and camera-to-world basis
+ * (columns right, up, back), as the viewer does each frame (main.cu:141-157). */
+gps_status gps_camera_from_pose(const float position[3], const float basis_cols[9],
+                                const gps_settings* settings, int32_t frame, gps_camera* cam);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GPS_B200_H */

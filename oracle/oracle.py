@@ -1,0 +1,158 @@
+"""ctypes wrapper of the CPU oracle (oracle/oracle.cpp) — TEST INFRASTRUCTURE ONLY.
+
+The oracle is the checker: tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg
+use it; the library never does.  Build with `make -C oracle` (done by __graft_entry__.build()).
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from ctypes import POINTER, byref, c_float, c_int, c_int32, c_uint32, c_uint64, c_void_p
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "_build", "liboracle.so")
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} missing: run `make -C {_HERE}`")
+        L = ctypes.CDLL(LIB_PATH)
+        L.oracle_create.restype = c_void_p
+        L.oracle_create.argtypes = [c_void_p, c_uint64, c_void_p, c_int]
+        L.oracle_free.argtypes = [c_void_p]
+        L.oracle_render_frame.argtypes = [c_void_p, c_void_p, c_void_p, c_void_p]
+        L.oracle_splat_workload.argtypes = [c_void_p, c_void_p, c_int, c_void_p, c_void_p, c_uint32, c_uint32, c_int]
+        L.oracle_preprocess.argtypes = [c_void_p, c_void_p, c_int, c_void_p, c_void_p, c_void_p]
+        L.oracle_get_buffer.argtypes = [c_void_p, c_void_p]
+        L.oracle_buffer_entries.restype = c_uint64
+        L.oracle_buffer_entries.argtypes = [c_void_p]
+        L.oracle_get_hiz.argtypes = [c_void_p, c_void_p]
+        L.oracle_hiz_size.restype = c_uint64
+        L.oracle_hiz_size.argtypes = [c_void_p]
+        L.oracle_last_workload.argtypes = [c_void_p, c_void_p, POINTER(c_uint32), POINTER(c_uint32)]
+        L.oracle_get_survivors.argtypes = [c_void_p, c_void_p, c_void_p]
+        L.oracle_get_blocks.argtypes = [c_void_p, c_void_p, POINTER(c_uint32), POINTER(c_uint32)]
+        L.oracle_kat.argtypes = [c_void_p] * 3 + [c_int] + [c_void_p] * 7
+        L.oracle_splat_index.argtypes = [c_void_p, c_void_p, c_void_p, c_int, c_int, c_int, c_void_p]
+        L.oracle_depth_key.argtypes = [c_void_p, c_int, c_float, c_float, c_void_p]
+        L.oracle_rgb36.argtypes = [c_void_p, c_int, c_void_p]
+        _lib = L
+    return _lib
+
+
+def _p(a: np.ndarray):
+    return a.ctypes.data_as(c_void_p)
+
+
+class Oracle:
+    """One scene + settings + frame state, rendered on the CPU with `threads` threads."""
+
+    def __init__(self, gaussians: np.ndarray, settings, threads: int = 1):
+        g = np.ascontiguousarray(gaussians, dtype=np.float32)
+        self._g = g
+        self.settings = settings
+        self.n = g.shape[0]
+        self._h = lib().oracle_create(_p(g), g.shape[0], ctypes.addressof(settings), threads)
+
+    def render(self, cam):
+        s = self.settings
+        img = np.zeros((s.height, s.width, 3), np.float32)
+        dep = np.zeros((s.height, s.width), np.float32)
+        lib().oracle_render_frame(self._h, ctypes.addressof(cam), _p(img), _p(dep))
+        return img, dep
+
+    def preprocess(self, cam, first_pass=True):
+        counts = np.zeros(self.n, np.uint32)
+        mask = np.zeros((self.n + 31) // 32, np.uint32)
+        colors = np.zeros((self.n, 3), np.float32)
+        lib().oracle_preprocess(self._h, ctypes.addressof(cam), int(first_pass), _p(counts), _p(mask), _p(colors))
+        return counts, mask, colors
+
+    def splat_workload(self, cam, frame_seed, surv_gid, surv_start, points, clear=True):
+        g = np.ascontiguousarray(surv_gid, np.uint32)
+        st = np.ascontiguousarray(surv_start, np.uint32)
+        lib().oracle_splat_workload(self._h, ctypes.addressof(cam), frame_seed, _p(g), _p(st), g.size, points, int(clear))
+
+    def buffer(self):
+        out = np.zeros(lib().oracle_buffer_entries(self._h), np.uint64)
+        lib().oracle_get_buffer(self._h, _p(out))
+        return out
+
+    def hiz(self):
+        out = np.zeros(lib().oracle_hiz_size(self._h), np.float32)
+        lib().oracle_get_hiz(self._h, _p(out))
+        return out
+
+    def workload(self):
+        pp = np.zeros(2, np.uint32)
+        sv = c_uint32()
+        tot = c_uint32()
+        lib().oracle_last_workload(self._h, _p(pp), byref(sv), byref(tot))
+        gid = np.zeros(sv.value, np.uint32)
+        start = np.zeros(sv.value, np.uint32)
+        lib().oracle_get_survivors(self._h, _p(gid), _p(start))
+        return {"points_pass": pp, "survivors": sv.value, "total": tot.value, "surv_gid": gid, "surv_start": start}
+
+    def blocks(self):
+        n = (self.n + 3) // 4 + 1
+        nodes = np.zeros(n * 6, np.float32)
+        pb = c_uint32()
+        cnt = c_uint32()
+        lib().oracle_get_blocks(self._h, _p(nodes), byref(pb), byref(cnt))
+        return nodes[: cnt.value * 6].reshape(-1, 6), pb.value
+
+    def close(self):
+        if self._h:
+            lib().oracle_free(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def kat(idx, frame, x):
+    idx = np.ascontiguousarray(idx, np.uint32)
+    frame = np.ascontiguousarray(frame, np.uint32)
+    x = np.ascontiguousarray(x, np.float32)
+    n = idx.size
+    out = {
+        "seed": np.zeros((n, 2), np.uint32),
+        "pcg": np.zeros((n, 2), np.uint32),
+        "pcgf": np.zeros((n, 2), np.float32),
+        "dilog": np.zeros(n, np.float32),
+        "invdilog": np.zeros(n, np.float32),
+        "poisson": np.zeros(n, np.uint32),
+        "sround": np.zeros(n, np.int32),
+    }
+    lib().oracle_kat(_p(idx), _p(frame), _p(x), n, _p(out["seed"]), _p(out["pcg"]), _p(out["pcgf"]), _p(out["dilog"]),
+                     _p(out["invdilog"]), _p(out["poisson"]), _p(out["sround"]))
+    return out
+
+
+def splat_index(xs, ys, ps, npass, width):
+    xs, ys, ps = (np.ascontiguousarray(v, np.int32) for v in (xs, ys, ps))
+    out = np.zeros(xs.size, np.int64)
+    lib().oracle_splat_index(_p(xs), _p(ys), _p(ps), xs.size, npass, width, _p(out))
+    return out
+
+
+def depth_key(d, near, far):
+    d = np.ascontiguousarray(d, np.float32)
+    out = np.zeros(d.size, np.uint64)
+    lib().oracle_depth_key(_p(d), d.size, near, far, _p(out))
+    return out
+
+
+def rgb36(rgb):
+    rgb = np.ascontiguousarray(rgb, np.float32).reshape(-1, 3)
+    out = np.zeros(rgb.shape[0], np.uint64)
+    lib().oracle_rgb36(_p(rgb), rgb.shape[0], _p(out))
+    return out
