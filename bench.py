@@ -43,6 +43,9 @@ def workload_spec(name: str):
     if name == "town16m":
         return dict(n=16_000_000, kind="town", width=1920, height=1080, ss=2, spp=4, reduce=1, hier=1, occl=1,
                     taa=1, frames=120)
+    if name == "town4m":  # profiling-size variant of the headline workload
+        return dict(n=4_000_000, kind="town", width=1920, height=1080, ss=2, spp=4, reduce=1, hier=1, occl=1,
+                    taa=1, frames=120)
     if name == "cube1m":
         return dict(n=1_000_000, kind="cube", width=640, height=360, ss=1, spp=1, reduce=1, hier=0, occl=0, taa=0,
                     frames=1)
@@ -237,7 +240,7 @@ def main():
     ap.add_argument("--steps", type=int, default=30)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="mine", choices=["mine", "reference"])
-    ap.add_argument("--workload", default="town16m", choices=["town16m", "cube1m"])
+    ap.add_argument("--workload", default="town16m", choices=["town16m", "town4m", "cube1m"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)

@@ -58,17 +58,6 @@ GPS_D vec3 color_from_sh_fp32(vec3 pos, vec3 campos, const float* shs) {
     return vmax0(result);
 }
 
-// a*b - c*d and a*b + c*d of the SH band recurrence with an explicit fused product
-#ifndef GPS_SH_FORM
-#define GPS_SH_FORM 32
-#endif
-GPS_D float sh_rec(float a, float b, float c, float d, bool minus, int bit) {
-    const float cd = minus ? -c : c;
-    if ((GPS_SH_FORM >> 5) & 1) return minus ? a * b - c * d : a * b + c * d;
-    if ((GPS_SH_FORM >> bit) & 1) return __fmaf_rn(cd, d, __fmul_rn(a, b));
-    return __fmaf_rn(a, b, __fmul_rn(cd, d));
-}
-
 // sh.cuh:55-96: real SH basis to band 3, Sloan's recurrence ordering
 GPS_D void eval_sh_basis_l3(float out[16], vec3 dir) {
     float x, y, z, z2, c0, s0, c1, s1, d, a, b;
@@ -98,34 +87,42 @@ GPS_D void eval_sh_basis_l3(float out[16], vec3 dir) {
     d = -2.285228997f * a;
     out[11] = s1 * d;
     out[13] = c1 * d;
-    c0 = sh_rec(x, c1, y, s1, true, 1);
-    s0 = sh_rec(y, c1, x, s1, false, 2);
+    c0 = x * c1 - y * s1;
+    s0 = y * c1 + x * s1;
     d = 0.546274215f;
     out[4] = s0 * d;
     out[8] = c0 * d;
     d = 1.445305721f * z;
     out[10] = s0 * d;
     out[14] = c0 * d;
-    c1 = sh_rec(x, c0, y, s0, true, 3);
-    s1 = sh_rec(y, c0, x, s0, false, 4);
+    c1 = x * c0 - y * s0;
+    s1 = y * c0 + x * s0;
     d = -0.59004359f;
     out[9] = s1 * d;
     out[15] = c1 * d;
 }
 
-// glm::mix(x, y, a) = x*(1-a) + y*a, per component.  Which of the two products nvcc fuses
-// into the multiply-add depends on the surrounding code, so the form is spelled out.
-#ifndef GPS_MIX_SITES
-#define GPS_MIX_SITES 0
-#endif
-template <int kSite>
-GPS_D float mixf_ref(float x, float y, float a) {
-    if ((GPS_MIX_SITES >> kSite) & 1) return __fmaf_rn(y, a, __fmul_rn(x, 1.0f - a));
+// glm::mix(x, y, a) = x*(1-a) + y*a.  In the reference build nvcc fuses one of the two
+// products into the multiply-add and keeps the other rounded, and which one differs per
+// vector component of the position and log-scale dequantisation (established by comparing
+// every Gaussian's decoded position against the reference kernels' outputs).  The two forms
+// are therefore written out explicitly:
+//   kFuseSecond: fma(y, a, round(x*(1-a)))      kFuseFirst: fma(x, 1-a, round(y*a))
+constexpr int kFuseFirst = 0, kFuseSecond = 1;
+template <int kForm>
+GPS_D float mix_form(float x, float y, float a) {
+    if (kForm == kFuseSecond) return __fmaf_rn(y, a, __fmul_rn(x, 1.0f - a));
     return __fmaf_rn(x, 1.0f - a, __fmul_rn(y, a));
 }
-template <int kSite>
-GPS_D vec3 mix3(vec3 x, vec3 y, vec3 a) {
-    return make_v3(mixf_ref<kSite>(x.x, y.x, a.x), mixf_ref<kSite>(x.y, y.y, a.y), mixf_ref<kSite>(x.z, y.z, a.z));
+// position and log-scale dequantisation (gaussian_types.cuh:346,371)
+GPS_D vec3 mix_dequant(vec3 x, vec3 y, vec3 a) {
+    return make_v3(mix_form<kFuseFirst>(x.x, y.x, a.x), mix_form<kFuseSecond>(x.y, y.y, a.y),
+                   mix_form<kFuseSecond>(x.z, y.z, a.z));
+}
+// compact SH dequantisation (sh.cuh:46)
+GPS_D vec3 mix_sh(vec3 x, vec3 y, vec3 a) {
+    return make_v3(mix_form<kFuseFirst>(x.x, y.x, a.x), mix_form<kFuseFirst>(x.y, y.y, a.y),
+                   mix_form<kFuseFirst>(x.z, y.z, a.z));
 }
 
 #endif  // __CUDACC__
@@ -193,7 +190,7 @@ struct SceneCompressed {
         float fx = float(px) / float((1u << 23) - 1u);
         float fy = float(py) / float((1u << 22) - 1u);
         float fz = float(pz) / float((1u << 23) - 1u);
-        mean = mix3<0>(bounds.min_pos, bounds.max_pos, make_v3(fx, fy, fz));
+        mean = mix_dequant(bounds.min_pos, bounds.max_pos, make_v3(fx, fy, fz));
 
         uint32_t rx = (q.z >> 4) & 0x3FFu;
         uint32_t ry = (q.z >> 14) & 0x3FFu;
@@ -215,7 +212,7 @@ struct SceneCompressed {
         uint32_t sy = (q.w >> 12) & 0x3FFu;
         uint32_t sz = (q.w >> 22) & 0x3FFu;
         vec3 st = make_v3((float)sx / 1023.0f, (float)sy / 1023.0f, (float)sz / 1023.0f);
-        vec3 ls = mix3<1>(bounds.min_scale, bounds.max_scale, st);
+        vec3 ls = mix_dequant(bounds.min_scale, bounds.max_scale, st);
         s = make_v3(__expf(ls.x), __expf(ls.y), __expf(ls.z));
     }
     // sh.cuh:257-273 with CompactSH::get (sh.cuh:41-47)
@@ -246,7 +243,7 @@ struct SceneCompressed {
             uint32_t q1 = (w[b1 >> 2] >> (8 * (b1 & 3))) & 0xFFu;
             uint32_t q2 = (w[b2 >> 2] >> (8 * (b2 & 3))) & 0xFFu;
             vec3 vq = make_v3((float)(int)q0 * r, (float)(int)q1 * r, (float)(int)q2 * r);
-            vec3 c = mix3<2>(bounds.min_sh[j], bounds.max_sh[j], vq);
+            vec3 c = mix_sh(bounds.min_sh[j], bounds.max_sh[j], vq);
             result = result + e[i] * c;
         }
         result = result + make_v3(0.5f, 0.5f, 0.5f);

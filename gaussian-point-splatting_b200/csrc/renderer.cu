@@ -869,8 +869,14 @@ gps_status gps_frame_loop_read(gps_frame_loop* l, uint8_t* host_rgb, void* strea
 
 gps_status gps_frame_loop_buffers(gps_frame_loop* l, int32_t slot, const uint8_t** d_u8, const float** d_color,
                                   const float** d_depth) {
-    if (!l || slot < 0 || slot > 1) return fail(GPS_ERR_INVALID_ARGUMENT, "bad argument");
+    if (!l || slot < 0 || slot > 2) return fail(GPS_ERR_INVALID_ARGUMENT, "bad argument");
     if (d_u8) *d_u8 = l->u8.get();
+    if (slot == 2) {
+        // resolved colour of the last frame before TAA blended it (TAA mode only)
+        if (d_color) *d_color = l->taa_out.get();
+        if (d_depth) *d_depth = nullptr;
+        return GPS_OK;
+    }
     if (d_color) *d_color = l->color[slot].get();
     if (d_depth) *d_depth = l->depth[slot].get();
     return GPS_OK;

@@ -204,7 +204,8 @@ gps_status gps_frame_loop_step(gps_frame_loop* l, const gps_camera* cam, void* s
 /* Copies the last u8 RGB frame (W*H*3 bytes) to host memory. */
 gps_status gps_frame_loop_read(gps_frame_loop* l, uint8_t* host_rgb, void* stream);
 /* Device buffers of ping-pong slot `slot` (0 or 1): frame f renders its colour into slot
- * f % 2 and its depth into slot 1 - f % 2 (render_server.cu:87-92). */
+ * f % 2 and its depth into slot 1 - f % 2 (render_server.cu:87-92).  Slot 2 (TAA mode):
+ * the last frame's resolved colour before TAA blended it (no depth). */
 gps_status gps_frame_loop_buffers(gps_frame_loop* l, int32_t slot, const uint8_t** d_u8, const float** d_color,
                                   const float** d_depth);
 

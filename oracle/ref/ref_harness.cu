@@ -208,6 +208,8 @@ static int run_render(int argc, char** argv) {
         int b = 1 - a;
         cudaEventRecord(ev0);
         gps->render(d_color[a], d_depth[b], s);
+        std::vector<float> pre_post;
+        if (dump_full && (int)fi < frames_to_dump) pre_post = d2h(reinterpret_cast<float*>(d_color[a]), size_t(W) * H * 3);
         {
             dim3 blockSize(256);
             dim3 gridSize((W * H + blockSize.x - 1) / blockSize.x);
@@ -268,6 +270,8 @@ static int run_render(int argc, char** argv) {
             std::vector<float> img = d2h(reinterpret_cast<float*>(d_color[a]), size_t(W) * H * 3);
             std::vector<float> dep = d2h(d_depth[b], size_t(W) * H);
             write_npy(P + "image.npy", img.data(), img.size(), "<f4", 4, {size_t(H), size_t(W), 3});
+            if (!pre_post.empty())
+                write_npy(P + "image_pre_post.npy", pre_post.data(), pre_post.size(), "<f4", 4, {size_t(H), size_t(W), 3});
             write_npy(P + "depth.npy", dep.data(), dep.size(), "<f4", 4, {size_t(H), size_t(W)});
             if (dump_post) {
                 std::vector<uint8_t> u8 = d2h(d_u8, size_t(W) * H * 3);

@@ -136,7 +136,8 @@ def run_reference(ply: str, settings, cams, variant="fp32", checksum_only=False,
     frames = []
     for i in range(len(cams)):
         d = {}
-        for name in ("derived", "buffer_checksum", "buffer", "image", "depth", "post_u8", "hiz", "offsets", "mask_last",
+        for name in ("derived", "buffer_checksum", "buffer", "image", "image_pre_post", "depth", "post_u8", "hiz",
+                     "offsets", "mask_last",
                      "mask_other", "indices", "colors", "stats", "culled"):
             p = os.path.join(out, f"f{i:03d}_{name}.npy")
             if os.path.exists(p):
@@ -173,6 +174,11 @@ def run_mine(scene, settings, cams, full=True):
         _, col_a, _ = loop.buffers(a)
         u8, _, dep_b = loop.buffers(1 - a)
         d["image"] = d2h(col_a, w * h * 3, np.float32).reshape(h, w, 3)
+        if settings.accumulation_mode == gpsplat.GPS_ACCUM_TAA:
+            _, pre, _ = loop.buffers(2)
+            d["image_pre_post"] = d2h(pre, w * h * 3, np.float32).reshape(h, w, 3)
+        else:
+            d["image_pre_post"] = d["image"]
         d["depth"] = d2h(dep_b, w * h, np.float32).reshape(h, w)
         d["post_u8"] = d2h(u8, w * h * 3, np.uint8).reshape(h, w, 3)
         v = r.debug_view()
