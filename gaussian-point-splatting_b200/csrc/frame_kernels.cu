@@ -13,8 +13,12 @@
 // value follows the reference's expression shape (see gps_math.cuh) so that the 64-bit
 // splat buffer is bit-identical to the reference kernels' for the same inputs.
 #include <cstdio>
+#include <mutex>
+#include <string>
+#include "../../include/gps_b200.h"
 #include "frame_kernels.h"
 #include "gps_rng.cuh"
+#include "host_io.hpp"
 
 namespace gps {
 
@@ -806,4 +810,91 @@ void launch_progressive(uint8_t* image, float* cur_color, float* accum, int widt
     progressive_kernel<<<(n + 255) / 256, 256, 0, stream>>>(image, cur_color, accum, width, height, frames);
 }
 
+// ---------------------------------------------------------------------------------
+// Allocation-free point scan.
+//
+// Some callers cannot allocate device memory at the moment they need the scan: code running
+// inside a CUDA-graph capture or a stream-ordered pipeline where cudaMalloc would synchronise
+// the device, a host with a fixed device-memory pool or budget enforced by its own allocator,
+// or a plugin host that owns every buffer and forbids its plugins from allocating. For them
+// the scan's only scratch — the decoupled look-back status word of every 4096-Gaussian tile
+// and the tile ticket — lives in this file-scope device array, and the caller passes all
+// inputs and outputs. The array is shared by every call on a device and keeps the previous
+// call's contents, so each call clears the part it uses first; calls that overlap on the GPU
+// (different streams, or host threads on the same device) race on it and must be serialised.
+// ---------------------------------------------------------------------------------
+constexpr uint32_t kNoAllocScanMaxTiles = 65536;  // 512 KiB of status words: n <= 2^28 Gaussians
+static __device__ __align__(256) unsigned long long g_noalloc_scan_scratch[kNoAllocScanMaxTiles + 1];
+
+namespace {
+constexpr int kNoAllocMaxDevices = 64;
+std::mutex g_noalloc_mutex;
+unsigned long long* g_noalloc_scratch_ptr[kNoAllocMaxDevices] = {};
+}  // namespace
+
 }  // namespace gps
+
+extern "C" gps_status gps_workload_scan_noalloc(const uint32_t* d_counts, const uint32_t* d_mask, uint32_t n,
+                                                uint32_t max_points, uint32_t* d_surv_gid, uint32_t* d_surv_start,
+                                                uint32_t* d_tile_first_rank, uint32_t* d_counters8, void* stream) {
+    using namespace gps;
+    const uint64_t tiles64 = ((uint64_t)n + kScanTile - 1) / kScanTile;
+    if (tiles64 > kNoAllocScanMaxTiles) {
+        set_last_error("gps_workload_scan_noalloc: " + std::to_string(n) + " Gaussians exceed the fixed scratch of " +
+                       std::to_string(kNoAllocScanMaxTiles) + " tiles (" +
+                       std::to_string((unsigned long long)kNoAllocScanMaxTiles * kScanTile) + " Gaussians)");
+        return GPS_ERR_SIZE;
+    }
+    const uint32_t tiles = (uint32_t)tiles64;
+    if ((n && (!d_counts || !d_mask || !d_surv_gid || !d_surv_start)) || !d_tile_first_rank || !d_counters8) {
+        set_last_error("gps_workload_scan_noalloc: null argument");
+        return GPS_ERR_INVALID_ARGUMENT;
+    }
+    if ((reinterpret_cast<uintptr_t>(d_counts) & 15u) != 0 || (reinterpret_cast<uintptr_t>(d_counters8) & 3u) != 0) {
+        set_last_error("gps_workload_scan_noalloc: d_counts must be 16-byte aligned, d_counters8 4-byte aligned");
+        return GPS_ERR_INVALID_ARGUMENT;
+    }
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess || dev < 0 || dev >= kNoAllocMaxDevices) {
+        set_last_error(std::string("gps_workload_scan_noalloc: no usable current device: ") + cudaGetErrorString(e));
+        return GPS_ERR_CUDA;
+    }
+    unsigned long long* scratch;
+    {
+        // Once per device, with that device current: the host-side name of a __device__
+        // array is not a device address, the address must be looked up.
+        std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+        if (!g_noalloc_scratch_ptr[dev]) {
+            void* p = nullptr;
+            e = cudaGetSymbolAddress(&p, g_noalloc_scan_scratch);
+            if (e != cudaSuccess) {
+                set_last_error(std::string("gps_workload_scan_noalloc: cudaGetSymbolAddress failed: ") + cudaGetErrorString(e));
+                return GPS_ERR_CUDA;
+            }
+            g_noalloc_scratch_ptr[dev] = static_cast<unsigned long long*>(p);
+        }
+        scratch = g_noalloc_scratch_ptr[dev];
+    }
+    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    ScanArgs a{};
+    a.counts = d_counts;
+    a.mask = d_mask;
+    a.n = n;
+    a.max_points = max_points;
+    a.tile_points = 256;
+    a.surv_gid = d_surv_gid;
+    a.surv_start = d_surv_start;
+    a.tile_first_rank = d_tile_first_rank;
+    a.tile_state = scratch;
+    // the ticket sits after the last status word a scan can use
+    a.tile_ticket = reinterpret_cast<uint32_t*>(scratch + kNoAllocScanMaxTiles);
+    a.counters = reinterpret_cast<PassCounters*>(d_counters8);
+    launch_scan(a, tiles, st);  // zeroes the status words, ticket and counters it uses, then scans
+    e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        set_last_error(std::string("gps_workload_scan_noalloc: ") + cudaGetErrorString(e));
+        return GPS_ERR_CUDA;
+    }
+    return GPS_OK;
+}
