@@ -139,16 +139,17 @@ __global__ void __launch_bounds__(256) block_cull_kernel(BlockView b, FrameConst
 // ---------------------------------------------------------------------------------
 // Preprocess (gaussian_point_splatting.cu:17-65 + 147-307)
 // ---------------------------------------------------------------------------------
+// One Gaussian: true if it splats this pass (record and count written).
 template <class Scene>
-__global__ void __launch_bounds__(256) preprocess_kernel(PreprocessArgs a, Scene scene) {
-    const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ bool preprocess_one(const PreprocessArgs& a, const Scene& scene, uint32_t gi) {
+    const int idx = (int)gi;
     const FrameConst& fc = a.fc;
-    u32x2 seed = make_seed((uint32_t)idx, (uint32_t)a.frame_seed);
     bool splats = false;
     do {
         if (idx >= (int)a.n) break;
         if (fc.enable_hier && block_culled(a.blocks, (uint32_t)idx)) break;
         if (a.only_previously_occluded && mask_bit(a.mask_prev, (uint32_t)idx)) break;
+        u32x2 seed = make_seed((uint32_t)idx, (uint32_t)a.frame_seed);
         float opacity = scene.opacity((uint32_t)idx);
         if (opacity <= 0.0f) break;
 
@@ -227,11 +228,21 @@ __global__ void __launch_bounds__(256) preprocess_kernel(PreprocessArgs a, Scene
         a.counts[idx] = num_points;
         splats = true;
     } while (false);
+    return splats;
+}
 
-    const unsigned m = __ballot_sync(0xffffffffu, splats);
-    if ((threadIdx.x & 31) == 0) {
-        const uint32_t warp_base = (uint32_t)idx & ~31u;
-        if (warp_base < a.n) a.mask_cur[warp_base >> 5] = m;
+// Persistent over 32-Gaussian chunks (one mask word each): a warp takes chunk after chunk, so
+// a pass over a mostly culled scene costs a bit test per Gaussian, not a thread-block launch
+// per 256 Gaussians.
+template <class Scene>
+__global__ void __launch_bounds__(256) preprocess_kernel(PreprocessArgs a, Scene scene) {
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t warps = gridDim.x * (blockDim.x >> 5);
+    const uint32_t chunks = (a.n + 31u) >> 5;
+    for (uint32_t c = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); c < chunks; c += warps) {
+        const bool splats = preprocess_one(a, scene, (c << 5) + lane);
+        const unsigned m = __ballot_sync(0xffffffffu, splats);
+        if (lane == 0) a.mask_cur[c] = m;
     }
 }
 
@@ -377,14 +388,34 @@ __global__ void __launch_bounds__(kScanThreads) scan_kernel(ScanArgs a) {
         if ((bits >> i) & 1u) {
             a.surv_gid[r] = base + i;
             a.surv_start[r] = pt;
-            // first survivor of every splat tile that starts inside [pt, pt + cnt) below the budget
-            unsigned long long lo = pt, hi = (unsigned long long)pt + cnt[i];
-            if (hi > a.max_points) hi = a.max_points;
-            unsigned long long t0 = (lo + a.tile_points - 1) / a.tile_points;
-            for (unsigned long long t = t0; t * a.tile_points < hi; ++t) a.tile_first_rank[t] = r;
             ++r;
             pt += cnt[i];
         }
+    }
+}
+
+// First survivor of every splat tile: tile t (points [t*tile_points, ...)) starts inside the
+// survivor with the largest rank whose first point is <= t*tile_points.  One thread per tile,
+// a binary search over the survivors' first points (monotone below 2^32 points per pass).  A
+// survivor can own thousands of tiles (a Gaussian right in front of the camera), so this is
+// done per tile rather than per survivor.
+__global__ void __launch_bounds__(256) tile_owner_kernel(const uint32_t* __restrict__ surv_start,
+                                                         uint32_t* __restrict__ tile_first_rank,
+                                                         const PassCounters* __restrict__ counters,
+                                                         uint32_t tile_points) {
+    const uint32_t points = counters->points;
+    const uint32_t survivors = counters->survivors;
+    if (points == 0 || survivors == 0) return;
+    const uint32_t tiles = (uint32_t)(((unsigned long long)points + tile_points - 1) / tile_points);
+    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < tiles; t += gridDim.x * blockDim.x) {
+        const uint32_t target = t * tile_points;
+        uint32_t lo = 0, hi = survivors - 1;
+        while (lo < hi) {
+            const uint32_t mid = lo + ((hi - lo + 1) >> 1);
+            if (__ldg(surv_start + mid) <= target) lo = mid;
+            else hi = mid - 1;
+        }
+        tile_first_rank[t] = lo;
     }
 }
 
@@ -410,8 +441,10 @@ __device__ __forceinline__ void atomic_add_color(unsigned long long* address, ui
     } while (assumed != old);
 }
 
-__device__ __forceinline__ void splat_point(uint32_t point, const SplatRecord& rec, const FrameConst& fc,
-                                            int frame_seed, uint64_t* __restrict__ buffer) {
+// Biased mode (use_unbiased_2d_splatting = false): samples in the reference's order, each
+// pre-tested and colour-added before the next one is drawn.
+__device__ __forceinline__ void splat_point_biased(uint32_t point, const SplatRecord& rec, const FrameConst& fc,
+                                                   int frame_seed, uint64_t* __restrict__ buffer) {
     u32x2 seed = make_seed(point, (uint32_t)frame_seed);
     const vec2 pixel_mean = make_v2(rec.a.x, rec.a.y);
     const float c0 = rec.a.z, c1 = rec.a.w, c2 = rec.b.x;
@@ -421,14 +454,11 @@ __device__ __forceinline__ void splat_point(uint32_t point, const SplatRecord& r
     const int maxx = (int)(rec.d.y & 0xFFFFu), maxy = (int)(rec.d.y >> 16);
     const uint64_t key = (uint64_t)rec.d.z | ((uint64_t)rec.d.w << 32);
     const uint64_t view_depth_bits = key & kDepthMask;
-    int k = fc.ss * fc.ss * kPointsPerKernel;
-    if (!fc.reduce_point_count) k = 1;
+    const int k = fc.k_points;
     const int samples = fc.num_passes * k;
     for (int p = 0; p < samples; ++p) {
         vec2 u = pcg2d(seed);
-        vec2 xy;
-        if (fc.use_unbiased) xy = corrected_box_muller(u.x, u.y, opacity);
-        else xy = box_muller(u.x, u.y);
+        vec2 xy = box_muller(u.x, u.y);
         vec2 pixel = make_v2(pixel_mean.x + c0 * xy.x, pixel_mean.y + c1 * xy.x + c2 * xy.y);
         pixel = make_v2(floorf(pixel.x), floorf(pixel.y));
         int x = (int)pixel.x;
@@ -441,8 +471,84 @@ __device__ __forceinline__ void splat_point(uint32_t point, const SplatRecord& r
         int index = splat_index(x, y, p / k, fc.num_passes, fc.up_width, fc.up_height);
         unsigned long long* slot = reinterpret_cast<unsigned long long*>(buffer + index);
         if ((uint64_t)__ldcg(slot) <= view_depth_bits) continue;
-        if (fc.use_unbiased) atomicMin(slot, (unsigned long long)key);
-        else atomic_add_color(slot, key);
+        atomic_add_color(slot, key);
+    }
+}
+
+// Unbiased mode (the default): the same sample stream, drawn kSplatBatch samples at a time.
+// Each batch computes its slots first, then issues their pre-test loads together (several
+// loads in flight per thread instead of one), then the atomicMins.  Order does not matter for
+// a min, and a slot is skipped only when it already holds a value <= this Gaussian's key, the
+// exact condition under which atomicMin would leave it unchanged (the reference skips when
+// the slot is <= the depth bits alone, a subset of these cases), so the buffer is identical.
+// Slot values only decrease during the kernel, so an L1-cached (possibly stale, hence larger)
+// pre-test value can only cause an extra atomic, never a wrong skip.
+#ifndef GPS_SPLAT_BATCH
+#define GPS_SPLAT_BATCH 4
+#endif
+constexpr int kSplatBatch = GPS_SPLAT_BATCH;
+
+__device__ __forceinline__ void splat_point_unbiased(uint32_t point, const SplatRecord& rec, const FrameConst& fc,
+                                                     int frame_seed, uint64_t* __restrict__ buffer) {
+    u32x2 seed = make_seed(point, (uint32_t)frame_seed);
+    const vec2 pixel_mean = make_v2(rec.a.x, rec.a.y);
+    const float c0 = rec.a.z, c1 = rec.a.w, c2 = rec.b.x;
+    const vec3 conic = make_v3(rec.b.y, rec.b.z, rec.b.w);
+    const float opacity = rec.c.x;
+    const int minx = (int)(rec.d.x & 0xFFFFu), miny = (int)(rec.d.x >> 16);
+    const int maxx = (int)(rec.d.y & 0xFFFFu), maxy = (int)(rec.d.y >> 16);
+    const unsigned long long key = (unsigned long long)rec.d.z | ((unsigned long long)rec.d.w << 32);
+    // the per-Gaussian factors of correctedBoxMuller (random.cuh:132-141), evaluated once
+    const float inv_alpha = 1.0f / fmaxf(opacity, 1.e-37f);
+    const float li2_alpha = dilog(opacity);
+    const int k = fc.k_points;
+    const int samples = fc.num_passes * k;
+    const int passes = fc.num_passes;
+    const int tiles_per_row = (fc.up_width + kTileSize - 1) >> kTileBits;
+    int p = 0, j = 0;
+    for (int s0 = 0; s0 < samples; s0 += kSplatBatch) {
+        uint32_t slot[kSplatBatch];
+        uint32_t live = 0;
+#pragma unroll
+        for (int b = 0; b < kSplatBatch; ++b) {
+            slot[b] = 0;
+            if (s0 + b < samples) {
+                vec2 u = pcg2d(seed);
+                float a = inv_alpha * inv_dilog((1.0f - u.x) * li2_alpha);
+                a = gclamp(a, 1.e-37f, 1.0f);
+                float r = __fsqrt_rn(fmaxf(-2.0f * __logf(a), 0.0f));
+                float theta = 2.0f * kPiF * u.y;
+                float sn, cs;
+                __sincosf(theta, &sn, &cs);
+                vec2 xy = make_v2(r * cs, r * sn);
+                vec2 pixel = make_v2(pixel_mean.x + c0 * xy.x, pixel_mean.y + c1 * xy.x + c2 * xy.y);
+                pixel = make_v2(floorf(pixel.x), floorf(pixel.y));
+                int x = (int)pixel.x;
+                int y = (int)pixel.y;
+                vec2 delta = make_v2(pixel_mean.x - pixel.x, pixel_mean.y - pixel.y);
+                if (x >= minx && x < maxx && y >= miny && y < maxy) {
+                    float alpha = opacity * gaussian_value(conic, delta);
+                    if (!(alpha < 1.0f / 255.0f)) {
+                        const uint32_t code = morton_encode((uint32_t)(x & (kTileSize - 1)), (uint32_t)(y & (kTileSize - 1)));
+                        const uint32_t tile = (uint32_t)((y >> kTileBits) * tiles_per_row + (x >> kTileBits));
+                        slot[b] = (tile * (uint32_t)(kTileSize * kTileSize) + code) * (uint32_t)passes + (uint32_t)p;
+                        live |= 1u << b;
+                    }
+                }
+                if (++j == k) {
+                    j = 0;
+                    ++p;
+                }
+            }
+        }
+        unsigned long long seen[kSplatBatch];
+#pragma unroll
+        for (int b = 0; b < kSplatBatch; ++b)
+            seen[b] = ((live >> b) & 1u) ? __ldca(reinterpret_cast<const unsigned long long*>(buffer) + slot[b]) : 0ull;
+#pragma unroll
+        for (int b = 0; b < kSplatBatch; ++b)
+            if (((live >> b) & 1u) && seen[b] > key)
+                atomicMin(reinterpret_cast<unsigned long long*>(buffer) + slot[b], key);
     }
 }
 
@@ -474,7 +580,8 @@ __global__ void __launch_bounds__(kSplatTile) splat_kernel(SplatArgs a) {
                 rec.b = __ldg(rp + 1);
                 rec.c = __ldg(rp + 2);
                 rec.d = __ldg(reinterpret_cast<const uint4*>(rp + 3));
-                splat_point(p, rec, a.fc, a.frame_seed, a.buffer);
+                if (a.fc.use_unbiased) splat_point_unbiased(p, rec, a.fc, a.frame_seed, a.buffer);
+                else splat_point_biased(p, rec, a.fc, a.frame_seed, a.buffer);
             }
         }
         __syncthreads();
@@ -490,11 +597,12 @@ __global__ void clear_kernel(ulonglong2* __restrict__ buf, uint64_t pairs, unsig
         buf[i] = v;
 }
 
+// One output pixel: the mean colour of its SS x SS x spp samples and their nearest NDC depth,
+// in the reference's loop order.  The depth arithmetic is kept in exactly this form (and
+// loop shape) because the reference's result depends on how the compiler evaluates it under
+// fast math; the parity tests check it bit for bit.
 template <bool kDepthOnly>
-__global__ void __launch_bounds__(256) resolve_kernel(ResolveArgs a) {
-    const int x = blockIdx.x * blockDim.x + threadIdx.x;
-    const int y = blockIdx.y * blockDim.y + threadIdx.y;
-    if (x >= a.width || y >= a.height) return;
+__device__ __forceinline__ void resolve_pixel(const ResolveArgs& a, int x, int y) {
     const uint32_t idx = (uint32_t)(y * a.width + x);
     const int bx = x * a.ss, by = y * a.ss;
     const int up_w = a.width * a.ss, up_h = a.height * a.ss;
@@ -505,7 +613,7 @@ __global__ void __launch_bounds__(256) resolve_kernel(ResolveArgs a) {
             for (int p = 0; p < a.num_passes; ++p) {
                 int i = splat_index(bx + dx, by + dy, p, a.num_passes, up_w, up_h);
                 if ((uint64_t)(int64_t)i >= a.entries) continue;
-                uint64_t val = __ldcs(reinterpret_cast<const unsigned long long*>(a.buffer) + i);
+                uint64_t val = __ldg(reinterpret_cast<const unsigned long long*>(a.buffer) + i);
                 float view_depth = view_depth_from_key((val >> 36ull) & kDepthMax, a.near_plane, a.far_plane);
                 float z_ndc = view_to_projected_depth(view_depth, a.near_plane, a.far_plane);
                 depth = gmin(depth, z_ndc);
@@ -523,36 +631,121 @@ __global__ void __launch_bounds__(256) resolve_kernel(ResolveArgs a) {
     a.depth[idx] = depth;
 }
 
+// Row-major pixels (any supersampling factor).
+template <bool kDepthOnly>
+__global__ void __launch_bounds__(256) resolve_kernel(ResolveArgs a) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y * blockDim.y + threadIdx.y;
+    if (x >= a.width || y >= a.height) return;
+    resolve_pixel<kDepthOnly>(a, x, y);
+}
+
+// Power-of-two supersampling: the pixels of each 64x64 splat tile in Morton order.  An
+// output pixel's sub-pixels are then one contiguous Morton range, its samples one contiguous
+// run of the buffer, and a warp reads 32 consecutive runs (4 KB at SS 2, 4 spp) instead of
+// runs scattered over a tile.
+__device__ __forceinline__ uint32_t morton_compact(uint32_t a) {
+    a &= 0x55555555u;
+    a = (a | (a >> 1)) & 0x33333333u;
+    a = (a | (a >> 2)) & 0x0F0F0F0Fu;
+    a = (a | (a >> 4)) & 0x00FF00FFu;
+    a = (a | (a >> 8)) & 0x0000FFFFu;
+    return a;
+}
+
+template <bool kDepthOnly>
+__global__ void __launch_bounds__(256) resolve_morton_kernel(ResolveArgs a, int ss_log2) {
+    const uint32_t tile_px = (uint32_t)kTileSize >> ss_log2;
+    const uint32_t per_tile_log2 = 2u * (uint32_t)(kTileBits - ss_log2);
+    const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t tile = g >> per_tile_log2;
+    const uint32_t m = g & ((1u << per_tile_log2) - 1u);
+    const uint32_t tiles_per_row = (uint32_t)((a.width * a.ss + kTileSize - 1) >> kTileBits);
+    const int x = (int)((tile % tiles_per_row) * tile_px + morton_compact(m));
+    const int y = (int)((tile / tiles_per_row) * tile_px + morton_compact(m >> 1));
+    if (x >= a.width || y >= a.height) return;
+    resolve_pixel<kDepthOnly>(a, x, y);
+}
+
 // ---------------------------------------------------------------------------------
 // Hi-Z chain (depth_mip_chain.cu:7-67)
 // ---------------------------------------------------------------------------------
-__global__ void hiz_blit_kernel(HizView c, const float* __restrict__ src) {
-    const int l = c.levels - 1;
-    const int wl = c.level_w[l], hl = c.level_h[l];
-    const int x = blockIdx.x * blockDim.x + threadIdx.x;
-    const int y = blockIdx.y * blockDim.y + threadIdx.y;
-    if (x >= wl || y >= hl) return;
-    c.mip[c.level_off[l] + (uint64_t)y * wl + x] = src[(uint64_t)y * wl + x];
-}
+// The whole chain in one launch.  Each 32x32-thread block copies a 32x32 tile of the depth
+// image into the finest level and reduces it through the next five levels in shared memory;
+// the block that finishes last (a counter, no waiting) reduces the remaining coarse levels.
+// Each texel is the min/max of the same finest texels as with one launch per level, so the
+// chain is identical.  Level j from the finest reduces with min while j <= min_levels.
+constexpr int kHizTile = 32;
 
-template <bool kMin>
-__global__ void hiz_reduce_kernel(HizView c, int l) {
-    const int wl = c.level_w[l], hl = c.level_h[l];
-    const int x = blockIdx.x * blockDim.x + threadIdx.x;
-    const int y = blockIdx.y * blockDim.y + threadIdx.y;
-    if (x >= wl || y >= hl) return;
-    const int wf = c.level_w[l + 1], hf = c.level_h[l + 1];
-    const float* fine = c.mip + c.level_off[l + 1];
-    float v = kMin ? INFINITY : -INFINITY;
-    for (int dy = 0; dy < 2; ++dy)
-        for (int dx = 0; dx < 2; ++dx) {
-            const int fx = 2 * x + dx, fy = 2 * y + dy;
-            if (fx < wf && fy < hf) {
-                float f = fine[(uint64_t)fy * wf + fx];
-                v = kMin ? fminf(v, f) : fmaxf(v, f);
-            }
+__global__ void __launch_bounds__(kHizTile * kHizTile) hiz_build_kernel(HizView c, const float* __restrict__ src,
+                                                                         int min_levels) {
+    __shared__ float sm[kHizTile * kHizTile];
+    __shared__ int s_last;
+    const int L = c.levels - 1;
+    const int tx = threadIdx.x & (kHizTile - 1), ty = threadIdx.x / kHizTile;
+    {
+        const int W = c.level_w[L], H = c.level_h[L];
+        const int x = blockIdx.x * kHizTile + tx, y = blockIdx.y * kHizTile + ty;
+        float v = 0.0f;
+        if (x < W && y < H) {
+            v = src[(uint64_t)y * W + x];
+            c.mip[c.level_off[L] + (uint64_t)y * W + x] = v;
         }
-    c.mip[c.level_off[l] + (uint64_t)y * wl + x] = v;
+        sm[ty * kHizTile + tx] = v;
+    }
+    __syncthreads();
+    const int local_levels = L < 5 ? L : 5;
+    for (int j = 1; j <= local_levels; ++j) {
+        const int l = L - j;
+        const bool use_min = (j - 1) < min_levels;
+        const int half = kHizTile >> j;
+        const int wf = c.level_w[l + 1], hf = c.level_h[l + 1];
+        const bool act = tx < half && ty < half;
+        const int gx = blockIdx.x * half + tx, gy = blockIdx.y * half + ty;
+        float r = use_min ? INFINITY : -INFINITY;
+        if (act) {
+            for (int dy = 0; dy < 2; ++dy)
+                for (int dx = 0; dx < 2; ++dx)
+                    if (2 * gx + dx < wf && 2 * gy + dy < hf) {
+                        const float f = sm[(2 * ty + dy) * kHizTile + 2 * tx + dx];
+                        r = use_min ? fminf(r, f) : fmaxf(r, f);
+                    }
+        }
+        __syncthreads();
+        if (act) {
+            sm[ty * kHizTile + tx] = r;
+            if (gx < c.level_w[l] && gy < c.level_h[l]) c.mip[c.level_off[l] + (uint64_t)gy * c.level_w[l] + gx] = r;
+        }
+        __syncthreads();
+    }
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) s_last = atomicAdd(c.done, 1u) == gridDim.x * gridDim.y - 1;
+    __syncthreads();
+    if (!s_last) return;
+    __threadfence();
+    for (int l = L - local_levels - 1; l >= 0; --l) {
+        const bool use_min = (L - 1 - l) < min_levels;
+        const int wl = c.level_w[l], hl = c.level_h[l];
+        const int wf = c.level_w[l + 1], hf = c.level_h[l + 1];
+        const float* fine = c.mip + c.level_off[l + 1];
+        for (int i = threadIdx.x; i < wl * hl; i += blockDim.x) {
+            const int x = i % wl, y = i / wl;
+            float r = use_min ? INFINITY : -INFINITY;
+            for (int dy = 0; dy < 2; ++dy)
+                for (int dx = 0; dx < 2; ++dx) {
+                    const int fx = 2 * x + dx, fy = 2 * y + dy;
+                    if (fx < wf && fy < hf) {
+                        const float f = __ldcg(fine + (uint64_t)fy * wf + fx);
+                        r = use_min ? fminf(r, f) : fmaxf(r, f);
+                    }
+                }
+            c.mip[c.level_off[l] + (uint64_t)y * wl + x] = r;
+        }
+        __threadfence_block();
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *c.done = 0u;
 }
 
 // ---------------------------------------------------------------------------------
@@ -721,14 +914,33 @@ void launch_block_cull(const BlockView& b, const FrameConst& fc, const HizView& 
     block_cull_kernel<<<(threads + 255) / 256, 256, 0, stream>>>(b, fc, hiz);
 }
 
+// Resident blocks of the persistent preprocess on this device, capped by the work.
+template <class Scene>
+int preprocess_grid_size(uint32_t n) {
+    static int per_sm = 0;
+    if (per_sm == 0) {
+        int blocks = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, preprocess_kernel<Scene>, 256, 0);
+        per_sm = blocks < 1 ? 1 : blocks;
+    }
+    if (g_num_sms == 0) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&g_num_sms, cudaDevAttrMultiProcessorCount, dev);
+    }
+    const uint64_t want = ((uint64_t)n + 255) / 256;
+    const uint64_t cap = (uint64_t)g_num_sms * (uint64_t)per_sm;
+    return (int)(want < cap ? want : cap);
+}
+
 void launch_preprocess_fp32(const PreprocessArgs& a, const SceneFP32& s, cudaStream_t stream) {
     if (a.n == 0) return;
-    preprocess_kernel<SceneFP32><<<(a.n + 255) / 256, 256, 0, stream>>>(a, s);
+    preprocess_kernel<SceneFP32><<<preprocess_grid_size<SceneFP32>(a.n), 256, 0, stream>>>(a, s);
 }
 
 void launch_preprocess_compressed(const PreprocessArgs& a, const SceneCompressed& s, cudaStream_t stream) {
     if (a.n == 0) return;
-    preprocess_kernel<SceneCompressed><<<(a.n + 255) / 256, 256, 0, stream>>>(a, s);
+    preprocess_kernel<SceneCompressed><<<preprocess_grid_size<SceneCompressed>(a.n), 256, 0, stream>>>(a, s);
 }
 
 uint32_t scan_tile_count(uint32_t n) { return (n + kScanTile - 1) / kScanTile; }
@@ -739,6 +951,10 @@ void launch_scan(const ScanArgs& a, uint32_t scan_tiles, cudaStream_t stream) {
     cudaMemsetAsync(a.counters, 0, sizeof(PassCounters), stream);
     if (scan_tiles == 0) return;
     scan_kernel<<<scan_tiles, kScanThreads, 0, stream>>>(a);
+    const uint64_t max_tiles = ((uint64_t)a.max_points + a.tile_points - 1) / a.tile_points;
+    const uint64_t want = (max_tiles + 255) / 256;
+    const int owner_grid = (int)(want < 1184 ? (want ? want : 1) : 1184);  // 148 SMs x 8
+    tile_owner_kernel<<<owner_grid, 256, 0, stream>>>(a.surv_start, a.tile_first_rank, a.counters, a.tile_points);
 }
 
 int splat_grid_size(int block) {
@@ -767,6 +983,18 @@ void launch_clear(uint64_t* buf, uint64_t entries, uint64_t value, cudaStream_t 
 }
 
 void launch_resolve(const ResolveArgs& a, bool depth_only, cudaStream_t stream) {
+    int ss_log2 = -1;
+    for (int l = 0; l <= 3; ++l)
+        if (a.ss == (1 << l)) ss_log2 = l;
+    if (ss_log2 >= 0) {
+        const uint64_t tiles = ((uint64_t)(a.width * a.ss + kTileSize - 1) >> kTileBits) *
+                               ((uint64_t)(a.height * a.ss + kTileSize - 1) >> kTileBits);
+        const uint64_t threads = tiles << (2 * (kTileBits - ss_log2));
+        const unsigned grid = (unsigned)((threads + 255) / 256);
+        if (depth_only) resolve_morton_kernel<true><<<grid, 256, 0, stream>>>(a, ss_log2);
+        else resolve_morton_kernel<false><<<grid, 256, 0, stream>>>(a, ss_log2);
+        return;
+    }
     dim3 block(16, 16);
     dim3 grid((a.width + 15) / 16, (a.height + 15) / 16);
     if (depth_only) resolve_kernel<true><<<grid, block, 0, stream>>>(a);
@@ -774,18 +1002,9 @@ void launch_resolve(const ResolveArgs& a, bool depth_only, cudaStream_t stream) 
 }
 
 void launch_hiz_build(const HizView& h, const float* depth, int min_levels, cudaStream_t stream) {
-    dim3 block(16, 16);
-    {
-        const int l = h.levels - 1;
-        dim3 grid((h.level_w[l] + 15) / 16, (h.level_h[l] + 15) / 16);
-        hiz_blit_kernel<<<grid, block, 0, stream>>>(h, depth);
-    }
-    for (int l = h.levels - 2; l >= 0; --l) {
-        dim3 grid((h.level_w[l] + 15) / 16, (h.level_h[l] + 15) / 16);
-        int from_finest = (h.levels - 2) - l;
-        if (from_finest < min_levels) hiz_reduce_kernel<true><<<grid, block, 0, stream>>>(h, l);
-        else hiz_reduce_kernel<false><<<grid, block, 0, stream>>>(h, l);
-    }
+    const int L = h.levels - 1;
+    dim3 grid((h.level_w[L] + kHizTile - 1) / kHizTile, (h.level_h[L] + kHizTile - 1) / kHizTile);
+    hiz_build_kernel<<<grid, kHizTile * kHizTile, 0, stream>>>(h, depth, min_levels);
 }
 
 void launch_block_bounds(const float4* pos_op, const float4* rot, const float4* scale, uint32_t n,

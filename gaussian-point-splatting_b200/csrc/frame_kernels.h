@@ -27,6 +27,7 @@ struct HizView {
     int level_w[16];
     int level_h[16];
     uint64_t level_off[16];
+    unsigned* done;        // block counter of the one-launch build (zero between builds)
 };
 
 // Fixed-size contiguous Gaussian blocks with AABBs (gaussian_bvh.cuh:8-53).

@@ -226,6 +226,7 @@ struct gps_renderer {
     dptr<unsigned long long> tile_state;
     dptr<PassCounters> counters;  // [2]: pass 1, pass 2
     dptr<float> mip;
+    dptr<unsigned> hiz_done;
     HizView hiz{};
     uint32_t scan_tiles = 0;
     uint32_t iteration = 0;
@@ -358,7 +359,7 @@ void render_pass(gps_renderer* r, const FrameConst& fc, int frame, bool first, c
     sa.tile_ticket = r->ticket.get();
     sa.counters = pc;
     launch_scan(sa, r->scan_tiles, st);
-    count_launch(r, kStScan, r->scan_tiles ? 1 : 0);
+    count_launch(r, kStScan, r->scan_tiles ? 2 : 0);  // scan + tile owners
     r->timer.mark(kStSplat, st);
     SplatArgs sp{};
     sp.fc = fc;
@@ -590,6 +591,9 @@ gps_status gps_renderer_create(gps_scene* scene, const gps_settings* settings, g
         hiz_layout(r->hiz, s.width, s.height);
         r->mip.reset(dev_alloc<float>(r->hiz.mip_size));
         r->hiz.mip = r->mip.get();
+        r->hiz_done.reset(dev_alloc<unsigned>(1));
+        GPS_CUDA(cudaMemset(r->hiz_done.get(), 0, sizeof(unsigned)));
+        r->hiz.done = r->hiz_done.get();
         // the reference leaves its Hi-Z uninitialised before the first frame; +inf here
         // means "nothing occluded" for frame 1
         fill_f32<<<148 * 4, 256>>>(r->mip.get(), r->hiz.mip_size, INFINITY);
@@ -641,7 +645,7 @@ gps_status gps_render_frame(gps_renderer* r, const gps_camera* cam, float* d_ima
         count_launch(r, kStResolve);
         r->timer.mark(kStHiz, st);
         launch_hiz_build(r->hiz, d_depth, r->s.occlusion_culling_min_reduce_count, st);
-        count_launch(r, kStHiz, (uint64_t)r->hiz.levels);
+        count_launch(r, kStHiz);
         if (r->n > 0) {
             render_pass(r, fc, cam->frame, false, st);
             r->second_pass_last = true;
@@ -655,7 +659,7 @@ gps_status gps_render_frame(gps_renderer* r, const gps_camera* cam, float* d_ima
     if (r->s.enable_occlusion_culling) {
         r->timer.mark(kStHiz, st);
         launch_hiz_build(r->hiz, d_depth, r->s.occlusion_culling_min_reduce_count, st);
-        count_launch(r, kStHiz, (uint64_t)r->hiz.levels);
+        count_launch(r, kStHiz);
     }
     r->timer.mark(-1, st);
     cudaMemcpyAsync(r->host_counters, r->counters.get(), sizeof(PassCounters) * 2, cudaMemcpyDeviceToHost, st);
