@@ -115,6 +115,7 @@ __device__ __forceinline__ bool aabb_project_bounds(vec3 bmin, vec3 bmax, const 
 
 __global__ void __launch_bounds__(256) block_cull_kernel(BlockView b, FrameConst fc, HizView hiz) {
     const uint32_t idx = blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx == 0 && b.chunk_count) *b.chunk_count = 0u;
     const uint32_t word = (idx & ~31u) >> 5;
     if (word >= b.words) return;
     bool culled = false;
@@ -134,6 +135,31 @@ __global__ void __launch_bounds__(256) block_cull_kernel(BlockView b, FrameConst
     __syncwarp();
     unsigned m = __ballot_sync(0xffffffffu, culled);
     if ((threadIdx.x & 31) == 0) b.culled[word] = m;
+}
+
+// Chunks of 32 Gaussians (one survivor-mask word each) that contain an unculled block, appended
+// warp by warp; culled chunks get their mask word zeroed here, since the preprocess skips them.
+__global__ void __launch_bounds__(256) visible_chunks_kernel(BlockView b, uint32_t n, uint32_t* __restrict__ list,
+                                                             uint32_t* __restrict__ mask_cur) {
+    const uint32_t chunks = (n + 31u) >> 5;
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t base = blockIdx.x * blockDim.x + (threadIdx.x & ~31u); base < chunks; base += stride) {
+        const uint32_t c = base + lane;
+        bool vis = false;
+        if (c < chunks) {
+            const uint32_t g1 = min((c << 5) + 31u, n - 1u);
+            for (uint32_t node = (c << 5) / b.per_block, last = g1 / b.per_block; node <= last && !vis; ++node)
+                vis = ((__ldg(&b.culled[node >> 5]) >> (node & 31u)) & 1u) == 0u;
+            if (!vis) mask_cur[c] = 0u;
+        }
+        const unsigned m = __ballot_sync(0xffffffffu, vis);
+        if (m == 0u) continue;
+        uint32_t slot = 0;
+        if (lane == (uint32_t)(__ffs(m) - 1)) slot = atomicAdd(b.chunk_count, (uint32_t)__popc(m));
+        slot = __shfl_sync(0xffffffffu, slot, __ffs(m) - 1);
+        if (vis) list[slot + (uint32_t)__popc(m & ((1u << lane) - 1u))] = c;
+    }
 }
 
 // ---------------------------------------------------------------------------------
@@ -238,8 +264,19 @@ template <class Scene>
 __global__ void __launch_bounds__(256) preprocess_kernel(PreprocessArgs a, Scene scene) {
     const uint32_t lane = threadIdx.x & 31u;
     const uint32_t warps = gridDim.x * (blockDim.x >> 5);
+    const uint32_t first = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    if (a.chunk_list) {
+        const uint32_t count = *a.chunk_count;
+        for (uint32_t i = first; i < count; i += warps) {
+            const uint32_t c = __ldg(a.chunk_list + i);
+            const bool splats = preprocess_one(a, scene, (c << 5) + lane);
+            const unsigned m = __ballot_sync(0xffffffffu, splats);
+            if (lane == 0) a.mask_cur[c] = m;
+        }
+        return;
+    }
     const uint32_t chunks = (a.n + 31u) >> 5;
-    for (uint32_t c = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); c < chunks; c += warps) {
+    for (uint32_t c = first; c < chunks; c += warps) {
         const bool splats = preprocess_one(a, scene, (c << 5) + lane);
         const unsigned m = __ballot_sync(0xffffffffu, splats);
         if (lane == 0) a.mask_cur[c] = m;
@@ -486,6 +523,12 @@ __device__ __forceinline__ void splat_point_biased(uint32_t point, const SplatRe
 #ifndef GPS_SPLAT_BATCH
 #define GPS_SPLAT_BATCH 4
 #endif
+// Pre-test before the atomic: 1 = L1-cached load, 2 = L2 load, 0 = none (every live sample
+// issues its atomicMin; the buffer is the same in all three).  On B200 the fire-and-forget
+// atomics alone measured fastest: the load adds latency to every sample and saves little L2 work.
+#ifndef GPS_SPLAT_PRETEST
+#define GPS_SPLAT_PRETEST 0
+#endif
 constexpr int kSplatBatch = GPS_SPLAT_BATCH;
 
 __device__ __forceinline__ void splat_point_unbiased(uint32_t point, const SplatRecord& rec, const FrameConst& fc,
@@ -541,17 +584,98 @@ __device__ __forceinline__ void splat_point_unbiased(uint32_t point, const Splat
                 }
             }
         }
+#if GPS_SPLAT_PRETEST
         unsigned long long seen[kSplatBatch];
 #pragma unroll
-        for (int b = 0; b < kSplatBatch; ++b)
-            seen[b] = ((live >> b) & 1u) ? __ldca(reinterpret_cast<const unsigned long long*>(buffer) + slot[b]) : 0ull;
+        for (int b = 0; b < kSplatBatch; ++b) {
+            const unsigned long long* at = reinterpret_cast<const unsigned long long*>(buffer) + slot[b];
+            seen[b] = ((live >> b) & 1u) ? (GPS_SPLAT_PRETEST == 1 ? __ldca(at) : __ldcg(at)) : 0ull;
+        }
 #pragma unroll
         for (int b = 0; b < kSplatBatch; ++b)
             if (((live >> b) & 1u) && seen[b] > key)
                 atomicMin(reinterpret_cast<unsigned long long*>(buffer) + slot[b], key);
+#else
+#pragma unroll
+        for (int b = 0; b < kSplatBatch; ++b)
+            if ((live >> b) & 1u) atomicMin(reinterpret_cast<unsigned long long*>(buffer) + slot[b], key);
+#endif
     }
 }
 
+// The same stream with K (points per thread per pass, ss*ss) known at compile time: the K
+// samples of a pass are drawn without branches (bounds and alpha tests become predicates), so
+// their independent transcendental chains can be interleaved, then the live ones are splatted.
+struct SampleConst {
+    vec2 pixel_mean;
+    float c0, c1, c2, opacity, inv_alpha, li2_alpha;
+    vec3 conic;
+    int minx, miny, maxx, maxy;
+    int tiles_per_row, passes;
+};
+
+__device__ __forceinline__ bool draw_sample(u32x2& seed, const SampleConst& c, int p, uint32_t& slot) {
+    const vec2 u = pcg2d(seed);
+    float a = c.inv_alpha * inv_dilog((1.0f - u.x) * c.li2_alpha);
+    a = gclamp(a, 1.e-37f, 1.0f);
+    const float r = __fsqrt_rn(fmaxf(-2.0f * __logf(a), 0.0f));
+    const float theta = 2.0f * kPiF * u.y;
+    float sn, cs;
+    __sincosf(theta, &sn, &cs);
+    const vec2 xy = make_v2(r * cs, r * sn);
+    vec2 pixel = make_v2(c.pixel_mean.x + c.c0 * xy.x, c.pixel_mean.y + c.c1 * xy.x + c.c2 * xy.y);
+    pixel = make_v2(floorf(pixel.x), floorf(pixel.y));
+    const int x = (int)pixel.x;
+    const int y = (int)pixel.y;
+    const vec2 delta = make_v2(c.pixel_mean.x - pixel.x, c.pixel_mean.y - pixel.y);
+    const bool inside = (x >= c.minx) & (x < c.maxx) & (y >= c.miny) & (y < c.maxy);
+    const float alpha = c.opacity * gaussian_value(c.conic, delta);
+    const uint32_t code = morton_encode((uint32_t)(x & (kTileSize - 1)), (uint32_t)(y & (kTileSize - 1)));
+    const uint32_t tile = (uint32_t)((y >> kTileBits) * c.tiles_per_row + (x >> kTileBits));
+    slot = (tile * (uint32_t)(kTileSize * kTileSize) + code) * (uint32_t)c.passes + (uint32_t)p;
+    return inside & !(alpha < 1.0f / 255.0f);
+}
+
+template <int K>
+__device__ __forceinline__ void splat_point_unbiased_k(uint32_t point, const SplatRecord& rec, const FrameConst& fc,
+                                                       int frame_seed, uint64_t* __restrict__ buffer) {
+    u32x2 seed = make_seed(point, (uint32_t)frame_seed);
+    SampleConst c;
+    c.pixel_mean = make_v2(rec.a.x, rec.a.y);
+    c.c0 = rec.a.z;
+    c.c1 = rec.a.w;
+    c.c2 = rec.b.x;
+    c.conic = make_v3(rec.b.y, rec.b.z, rec.b.w);
+    c.opacity = rec.c.x;
+    c.minx = (int)(rec.d.x & 0xFFFFu);
+    c.miny = (int)(rec.d.x >> 16);
+    c.maxx = (int)(rec.d.y & 0xFFFFu);
+    c.maxy = (int)(rec.d.y >> 16);
+    // the per-Gaussian factors of correctedBoxMuller (random.cuh:132-141), evaluated once
+    c.inv_alpha = 1.0f / fmaxf(c.opacity, 1.e-37f);
+    c.li2_alpha = dilog(c.opacity);
+    c.passes = fc.num_passes;
+    c.tiles_per_row = (fc.up_width + kTileSize - 1) >> kTileBits;
+    const unsigned long long key = (unsigned long long)rec.d.z | ((unsigned long long)rec.d.w << 32);
+    unsigned long long* buf = reinterpret_cast<unsigned long long*>(buffer);
+    for (int p = 0; p < c.passes; ++p) {
+        uint32_t slot[K];
+        bool live[K];
+#pragma unroll
+        for (int j = 0; j < K; ++j) live[j] = draw_sample(seed, c, p, slot[j]);
+#pragma unroll
+        for (int j = 0; j < K; ++j) {
+#if GPS_SPLAT_PRETEST
+            if (live[j] && (GPS_SPLAT_PRETEST == 1 ? __ldca(buf + slot[j]) : __ldcg(buf + slot[j])) > key) atomicMin(buf + slot[j], key);
+#else
+            if (live[j]) atomicMin(buf + slot[j], key);
+#endif
+        }
+    }
+}
+
+// K > 0: unbiased splatting with K points per thread per pass; K = 0: any other setting.
+template <int K>
 __global__ void __launch_bounds__(kSplatTile) splat_kernel(SplatArgs a) {
     __shared__ uint32_t s_start[kSplatTile];
     const uint32_t points = a.counters->points;
@@ -580,8 +704,12 @@ __global__ void __launch_bounds__(kSplatTile) splat_kernel(SplatArgs a) {
                 rec.b = __ldg(rp + 1);
                 rec.c = __ldg(rp + 2);
                 rec.d = __ldg(reinterpret_cast<const uint4*>(rp + 3));
-                if (a.fc.use_unbiased) splat_point_unbiased(p, rec, a.fc, a.frame_seed, a.buffer);
-                else splat_point_biased(p, rec, a.fc, a.frame_seed, a.buffer);
+                if constexpr (K > 0) {
+                    splat_point_unbiased_k<K>(p, rec, a.fc, a.frame_seed, a.buffer);
+                } else {
+                    if (a.fc.use_unbiased) splat_point_unbiased(p, rec, a.fc, a.frame_seed, a.buffer);
+                    else splat_point_biased(p, rec, a.fc, a.frame_seed, a.buffer);
+                }
             }
         }
         __syncthreads();
@@ -597,12 +725,29 @@ __global__ void clear_kernel(ulonglong2* __restrict__ buf, uint64_t pairs, unsig
         buf[i] = v;
 }
 
+// Where resolve_pixel reads entry i of the splat buffer from.
+struct GlobalEntries {
+    const uint64_t* buffer;
+    __device__ __forceinline__ uint64_t operator()(int i) const {
+        return __ldg(reinterpret_cast<const unsigned long long*>(buffer) + i);
+    }
+};
+struct StagedEntries {  // a contiguous run of the buffer copied to shared memory, one pad
+    const uint64_t* stage;  // word after every pixel's samples (stride = run + 1)
+    int first;
+    int run_log2;
+    __device__ __forceinline__ uint64_t operator()(int i) const {
+        const int w = i - first;
+        return stage[w + (w >> run_log2)];
+    }
+};
+
 // One output pixel: the mean colour of its SS x SS x spp samples and their nearest NDC depth,
 // in the reference's loop order.  The depth arithmetic is kept in exactly this form (and
 // loop shape) because the reference's result depends on how the compiler evaluates it under
 // fast math; the parity tests check it bit for bit.
-template <bool kDepthOnly>
-__device__ __forceinline__ void resolve_pixel(const ResolveArgs& a, int x, int y) {
+template <bool kDepthOnly, class Src>
+__device__ __forceinline__ void resolve_pixel(const ResolveArgs& a, int x, int y, Src src) {
     const uint32_t idx = (uint32_t)(y * a.width + x);
     const int bx = x * a.ss, by = y * a.ss;
     const int up_w = a.width * a.ss, up_h = a.height * a.ss;
@@ -613,7 +758,7 @@ __device__ __forceinline__ void resolve_pixel(const ResolveArgs& a, int x, int y
             for (int p = 0; p < a.num_passes; ++p) {
                 int i = splat_index(bx + dx, by + dy, p, a.num_passes, up_w, up_h);
                 if ((uint64_t)(int64_t)i >= a.entries) continue;
-                uint64_t val = __ldg(reinterpret_cast<const unsigned long long*>(a.buffer) + i);
+                uint64_t val = src(i);
                 float view_depth = view_depth_from_key((val >> 36ull) & kDepthMax, a.near_plane, a.far_plane);
                 float z_ndc = view_to_projected_depth(view_depth, a.near_plane, a.far_plane);
                 depth = gmin(depth, z_ndc);
@@ -637,7 +782,7 @@ __global__ void __launch_bounds__(256) resolve_kernel(ResolveArgs a) {
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     const int y = blockIdx.y * blockDim.y + threadIdx.y;
     if (x >= a.width || y >= a.height) return;
-    resolve_pixel<kDepthOnly>(a, x, y);
+    resolve_pixel<kDepthOnly>(a, x, y, GlobalEntries{a.buffer});
 }
 
 // Power-of-two supersampling: the pixels of each 64x64 splat tile in Morton order.  An
@@ -664,83 +809,162 @@ __global__ void __launch_bounds__(256) resolve_morton_kernel(ResolveArgs a, int 
     const int x = (int)((tile % tiles_per_row) * tile_px + morton_compact(m));
     const int y = (int)((tile / tiles_per_row) * tile_px + morton_compact(m >> 1));
     if (x >= a.width || y >= a.height) return;
-    resolve_pixel<kDepthOnly>(a, x, y);
+    resolve_pixel<kDepthOnly>(a, x, y, GlobalEntries{a.buffer});
+}
+
+// Staged variant: a block's pixels are consecutive in Morton-tile order, so their samples are
+// one contiguous run of the buffer (px_per_block x SS*SS*spp entries, at most 48 KB).  The
+// block copies the run to shared memory with coalesced 16-byte loads, all in flight at once,
+// then each thread resolves its pixel from shared memory with the same per-pixel code.  A pad
+// word after each pixel's samples keeps the threads of a warp, which read samples a whole
+// pixel run apart, on different banks.  Used when SS*SS*spp is a power of two >= 2.
+constexpr int kResolveStageBytes = 48 * 1024;
+
+template <bool kDepthOnly>
+__global__ void __launch_bounds__(256) resolve_staged_kernel(ResolveArgs a, int ss_log2, int run_log2) {
+    extern __shared__ uint64_t stage[];
+    const uint32_t run = 1u << run_log2;                            // entries per pixel
+    const uint32_t g0 = blockIdx.x * blockDim.x;
+    const uint64_t first = (uint64_t)g0 * run;
+    uint64_t last = first + (uint64_t)blockDim.x * run;
+    if (last > a.entries) last = a.entries;
+    const uint32_t chunks = (uint32_t)((last - first) / 2);        // first and last are even
+    const ulonglong2* src = reinterpret_cast<const ulonglong2*>(a.buffer + first);
+    for (uint32_t i = threadIdx.x; i < chunks; i += blockDim.x) {
+        const ulonglong2 q = __ldcs(src + i);
+        const uint32_t w = 2u * i;                                  // both words in one pixel run
+        const uint32_t d = w + (w >> run_log2);
+        stage[d] = q.x;
+        stage[d + 1] = q.y;
+    }
+    __syncthreads();
+    const uint32_t tile_px = (uint32_t)kTileSize >> ss_log2;
+    const uint32_t per_tile_log2 = 2u * (uint32_t)(kTileBits - ss_log2);
+    const uint32_t g = g0 + threadIdx.x;
+    const uint32_t tile = g >> per_tile_log2;
+    const uint32_t m = g & ((1u << per_tile_log2) - 1u);
+    const uint32_t tiles_per_row = (uint32_t)((a.width * a.ss + kTileSize - 1) >> kTileBits);
+    const int x = (int)((tile % tiles_per_row) * tile_px + morton_compact(m));
+    const int y = (int)((tile / tiles_per_row) * tile_px + morton_compact(m >> 1));
+    if (x >= a.width || y >= a.height) return;
+    resolve_pixel<kDepthOnly>(a, x, y, StagedEntries{stage, (int)first, run_log2});
 }
 
 // ---------------------------------------------------------------------------------
 // Hi-Z chain (depth_mip_chain.cu:7-67)
 // ---------------------------------------------------------------------------------
-// The whole chain in one launch.  Each 32x32-thread block copies a 32x32 tile of the depth
-// image into the finest level and reduces it through the next five levels in shared memory;
-// the block that finishes last (a counter, no waiting) reduces the remaining coarse levels.
-// Each texel is the min/max of the same finest texels as with one launch per level, so the
-// chain is identical.  Level j from the finest reduces with min while j <= min_levels.
-constexpr int kHizTile = 32;
+// The whole chain in one launch.  A 16x16-thread block covers a 64x64 tile of the depth image:
+// each thread copies its 4x4 texels into the finest level and reduces them in registers to
+// the next two levels (2x2, then 1), the block reduces its 16x16 results through four more
+// levels in shared memory, and the block that finishes last (a counter, no waiting) reduces
+// the remaining coarse levels.  Every texel is the min/max of the same finest texels as with
+// one launch per level, so the chain is identical.  Level j from the finest (j = 1, 2, ...)
+// reduces with min while j <= min_levels, else with max.
+constexpr int kHizThreads = 16;                  // threads per block edge
+constexpr int kHizTile = 4 * kHizThreads;        // finest texels per block edge
 
-__global__ void __launch_bounds__(kHizTile * kHizTile) hiz_build_kernel(HizView c, const float* __restrict__ src,
-                                                                         int min_levels) {
-    __shared__ float sm[kHizTile * kHizTile];
+__device__ __forceinline__ float hiz_op(bool use_min, float a, float b) { return use_min ? fminf(a, b) : fmaxf(a, b); }
+
+__global__ void __launch_bounds__(kHizThreads * kHizThreads) hiz_build_kernel(HizView c, const float* __restrict__ src,
+                                                                               int min_levels) {
+    __shared__ float sm[kHizThreads * kHizThreads];
     __shared__ int s_last;
     const int L = c.levels - 1;
-    const int tx = threadIdx.x & (kHizTile - 1), ty = threadIdx.x / kHizTile;
-    {
-        const int W = c.level_w[L], H = c.level_h[L];
-        const int x = blockIdx.x * kHizTile + tx, y = blockIdx.y * kHizTile + ty;
-        float v = 0.0f;
-        if (x < W && y < H) {
-            v = src[(uint64_t)y * W + x];
-            c.mip[c.level_off[L] + (uint64_t)y * W + x] = v;
+    const int tx = threadIdx.x % kHizThreads, ty = threadIdx.x / kHizThreads;
+    const int gx = blockIdx.x * kHizThreads + tx, gy = blockIdx.y * kHizThreads + ty;  // coords at level L-2
+    const int W = c.level_w[L], H = c.level_h[L];
+    float f[4][4];
+#pragma unroll
+    for (int v = 0; v < 4; ++v)
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int x = 4 * gx + u, y = 4 * gy + v;
+            f[v][u] = 0.0f;
+            if (x < W && y < H) {
+                f[v][u] = src[(uint64_t)y * W + x];
+                c.mip[c.level_off[L] + (uint64_t)y * W + x] = f[v][u];
+            }
         }
-        sm[ty * kHizTile + tx] = v;
+    float r = 0.0f;  // this thread's texel at the last level reduced so far
+    bool have = false;
+    if (L >= 1) {
+        const int l = L - 1;
+        const bool use_min = 0 < min_levels;
+        const int wl = c.level_w[l], hl = c.level_h[l];
+        float q[2][2];
+#pragma unroll
+        for (int j = 0; j < 2; ++j)
+#pragma unroll
+            for (int i = 0; i < 2; ++i) {
+                float acc = use_min ? INFINITY : -INFINITY;
+#pragma unroll
+                for (int dy = 0; dy < 2; ++dy)
+#pragma unroll
+                    for (int dx = 0; dx < 2; ++dx)
+                        if (4 * gx + 2 * i + dx < W && 4 * gy + 2 * j + dy < H) acc = hiz_op(use_min, acc, f[2 * j + dy][2 * i + dx]);
+                q[j][i] = acc;
+                const int x = 2 * gx + i, y = 2 * gy + j;
+                if (x < wl && y < hl) c.mip[c.level_off[l] + (uint64_t)y * wl + x] = acc;
+            }
+        if (L >= 2) {
+            const int l2 = L - 2;
+            const bool use_min2 = 1 < min_levels;
+            float acc = use_min2 ? INFINITY : -INFINITY;
+#pragma unroll
+            for (int j = 0; j < 2; ++j)
+#pragma unroll
+                for (int i = 0; i < 2; ++i)
+                    if (2 * gx + i < wl && 2 * gy + j < hl) acc = hiz_op(use_min2, acc, q[j][i]);
+            r = acc;
+            have = true;
+            if (gx < c.level_w[l2] && gy < c.level_h[l2]) c.mip[c.level_off[l2] + (uint64_t)gy * c.level_w[l2] + gx] = acc;
+        }
     }
+    const int shared_levels = have ? min(4, L - 2) : 0;   // levels L-3 .. L-6 in shared memory
+    if (have) sm[ty * kHizThreads + tx] = r;
     __syncthreads();
-    const int local_levels = L < 5 ? L : 5;
-    for (int j = 1; j <= local_levels; ++j) {
-        const int l = L - j;
-        const bool use_min = (j - 1) < min_levels;
-        const int half = kHizTile >> j;
+    for (int j = 1; j <= shared_levels; ++j) {
+        const int l = L - 2 - j;
+        const bool use_min = (j + 1) < min_levels;
+        const int half = kHizThreads >> j;
         const int wf = c.level_w[l + 1], hf = c.level_h[l + 1];
         const bool act = tx < half && ty < half;
-        const int gx = blockIdx.x * half + tx, gy = blockIdx.y * half + ty;
-        float r = use_min ? INFINITY : -INFINITY;
+        const int bx = blockIdx.x * half + tx, by = blockIdx.y * half + ty;
+        float acc = use_min ? INFINITY : -INFINITY;
         if (act) {
             for (int dy = 0; dy < 2; ++dy)
                 for (int dx = 0; dx < 2; ++dx)
-                    if (2 * gx + dx < wf && 2 * gy + dy < hf) {
-                        const float f = sm[(2 * ty + dy) * kHizTile + 2 * tx + dx];
-                        r = use_min ? fminf(r, f) : fmaxf(r, f);
-                    }
+                    if (2 * bx + dx < wf && 2 * by + dy < hf) acc = hiz_op(use_min, acc, sm[(2 * ty + dy) * kHizThreads + 2 * tx + dx]);
         }
         __syncthreads();
         if (act) {
-            sm[ty * kHizTile + tx] = r;
-            if (gx < c.level_w[l] && gy < c.level_h[l]) c.mip[c.level_off[l] + (uint64_t)gy * c.level_w[l] + gx] = r;
+            sm[ty * kHizThreads + tx] = acc;
+            if (bx < c.level_w[l] && by < c.level_h[l]) c.mip[c.level_off[l] + (uint64_t)by * c.level_w[l] + bx] = acc;
         }
         __syncthreads();
     }
+    const int done_levels = (L >= 2 ? 2 : L) + shared_levels;   // levels below L written so far
+    if (done_levels >= L) return;                                // the whole chain fits one block
     __threadfence();
     __syncthreads();
     if (threadIdx.x == 0) s_last = atomicAdd(c.done, 1u) == gridDim.x * gridDim.y - 1;
     __syncthreads();
     if (!s_last) return;
     __threadfence();
-    for (int l = L - local_levels - 1; l >= 0; --l) {
+    for (int l = L - done_levels - 1; l >= 0; --l) {
         const bool use_min = (L - 1 - l) < min_levels;
         const int wl = c.level_w[l], hl = c.level_h[l];
         const int wf = c.level_w[l + 1], hf = c.level_h[l + 1];
         const float* fine = c.mip + c.level_off[l + 1];
         for (int i = threadIdx.x; i < wl * hl; i += blockDim.x) {
             const int x = i % wl, y = i / wl;
-            float r = use_min ? INFINITY : -INFINITY;
+            float acc = use_min ? INFINITY : -INFINITY;
             for (int dy = 0; dy < 2; ++dy)
                 for (int dx = 0; dx < 2; ++dx) {
                     const int fx = 2 * x + dx, fy = 2 * y + dy;
-                    if (fx < wf && fy < hf) {
-                        const float f = __ldcg(fine + (uint64_t)fy * wf + fx);
-                        r = use_min ? fminf(r, f) : fmaxf(r, f);
-                    }
+                    if (fx < wf && fy < hf) acc = hiz_op(use_min, acc, __ldcg(fine + (uint64_t)fy * wf + fx));
                 }
-            c.mip[c.level_off[l] + (uint64_t)y * wl + x] = r;
+            c.mip[c.level_off[l] + (uint64_t)y * wl + x] = acc;
         }
         __threadfence_block();
         __syncthreads();
@@ -901,7 +1125,6 @@ __global__ void progressive_kernel(uint8_t* __restrict__ image, float* __restric
 }
 
 int g_num_sms = 0;
-int g_splat_blocks_per_sm = 0;
 
 }  // namespace
 
@@ -912,6 +1135,13 @@ void launch_block_cull(const BlockView& b, const FrameConst& fc, const HizView& 
     if (b.node_count == 0) return;
     uint32_t threads = b.words * 32;
     block_cull_kernel<<<(threads + 255) / 256, 256, 0, stream>>>(b, fc, hiz);
+}
+
+void launch_visible_chunks(const BlockView& b, uint32_t n, uint32_t* list, uint32_t* mask_cur, cudaStream_t stream) {
+    if (n == 0) return;
+    const uint32_t chunks = (n + 31u) >> 5;
+    const uint32_t want = (chunks + 255u) / 256u;
+    visible_chunks_kernel<<<want < 1184u ? want : 1184u, 256, 0, stream>>>(b, n, list, mask_cur);
 }
 
 // Resident blocks of the persistent preprocess on this device, capped by the work.
@@ -957,20 +1187,37 @@ void launch_scan(const ScanArgs& a, uint32_t scan_tiles, cudaStream_t stream) {
     tile_owner_kernel<<<owner_grid, 256, 0, stream>>>(a.surv_start, a.tile_first_rank, a.counters, a.tile_points);
 }
 
+template <int K>
+int splat_blocks_per_sm() {
+    static int per_sm = 0;
+    if (per_sm == 0) {
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, splat_kernel<K>, kSplatTile, 0);
+        if (per_sm < 1) per_sm = 1;
+    }
+    return per_sm;
+}
+
 int splat_grid_size(int block) {
+    (void)block;
     if (g_num_sms == 0) {
         int dev = 0;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&g_num_sms, cudaDevAttrMultiProcessorCount, dev);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&g_splat_blocks_per_sm, splat_kernel, block, 0);
-        if (g_splat_blocks_per_sm < 1) g_splat_blocks_per_sm = 1;
     }
-    return g_num_sms * g_splat_blocks_per_sm;
+    return g_num_sms * splat_blocks_per_sm<0>();
 }
 
 void launch_splat(const SplatArgs& a, int grid, int block, cudaStream_t stream) {
     (void)block;
-    splat_kernel<<<grid, kSplatTile, 0, stream>>>(a);
+    if (g_num_sms == 0) splat_grid_size(kSplatTile);
+    // a persistent grid: as many blocks as fit on the device at once
+    if (a.fc.use_unbiased && a.fc.k_points == 4) {
+        splat_kernel<4><<<g_num_sms * splat_blocks_per_sm<4>(), kSplatTile, 0, stream>>>(a);
+    } else if (a.fc.use_unbiased && a.fc.k_points == 1) {
+        splat_kernel<1><<<g_num_sms * splat_blocks_per_sm<1>(), kSplatTile, 0, stream>>>(a);
+    } else {
+        splat_kernel<0><<<grid, kSplatTile, 0, stream>>>(a);
+    }
 }
 
 void launch_clear(uint64_t* buf, uint64_t entries, uint64_t value, cudaStream_t stream) {
@@ -990,6 +1237,20 @@ void launch_resolve(const ResolveArgs& a, bool depth_only, cudaStream_t stream) 
         const uint64_t tiles = ((uint64_t)(a.width * a.ss + kTileSize - 1) >> kTileBits) *
                                ((uint64_t)(a.height * a.ss + kTileSize - 1) >> kTileBits);
         const uint64_t threads = tiles << (2 * (kTileBits - ss_log2));
+        const uint32_t run = (uint32_t)(a.ss * a.ss * a.num_passes);
+        int run_log2 = -1;
+        for (int l = 1; l <= 12; ++l)
+            if (run == (1u << l)) run_log2 = l;
+        const uint32_t run_bytes = (run + 1u) * 8u;                 // with the pad word
+        uint32_t px = 256;
+        while (px > 32 && px * run_bytes > (uint32_t)kResolveStageBytes) px >>= 1;
+        if (run_log2 > 0 && px * run_bytes <= (uint32_t)kResolveStageBytes && (uint64_t)a.entries <= 0x7FFFFFFFull) {
+            const unsigned grid = (unsigned)((threads + px - 1) / px);
+            const size_t smem = (size_t)px * run_bytes;
+            if (depth_only) resolve_staged_kernel<true><<<grid, px, smem, stream>>>(a, ss_log2, run_log2);
+            else resolve_staged_kernel<false><<<grid, px, smem, stream>>>(a, ss_log2, run_log2);
+            return;
+        }
         const unsigned grid = (unsigned)((threads + 255) / 256);
         if (depth_only) resolve_morton_kernel<true><<<grid, 256, 0, stream>>>(a, ss_log2);
         else resolve_morton_kernel<false><<<grid, 256, 0, stream>>>(a, ss_log2);
@@ -1004,7 +1265,7 @@ void launch_resolve(const ResolveArgs& a, bool depth_only, cudaStream_t stream) 
 void launch_hiz_build(const HizView& h, const float* depth, int min_levels, cudaStream_t stream) {
     const int L = h.levels - 1;
     dim3 grid((h.level_w[L] + kHizTile - 1) / kHizTile, (h.level_h[L] + kHizTile - 1) / kHizTile);
-    hiz_build_kernel<<<grid, kHizTile * kHizTile, 0, stream>>>(h, depth, min_levels);
+    hiz_build_kernel<<<grid, kHizThreads * kHizThreads, 0, stream>>>(h, depth, min_levels);
 }
 
 void launch_block_bounds(const float4* pos_op, const float4* rot, const float4* scale, uint32_t n,

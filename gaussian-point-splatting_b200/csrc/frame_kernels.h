@@ -37,6 +37,7 @@ struct BlockView {
     uint32_t node_count;
     uint32_t words;
     uint32_t per_block;    // Gaussians per block
+    uint32_t* chunk_count; // visible-chunk counter, reset by the block cull
 };
 
 // Device-side counters of one render pass, readable by later kernels without a host sync.
@@ -77,6 +78,8 @@ struct PreprocessArgs {
     SplatRecord* records;
     HizView hiz;
     BlockView blocks;
+    const uint32_t* chunk_list;   // 32-Gaussian chunks with a visible block (null: every chunk)
+    const uint32_t* chunk_count;
 };
 
 struct ScanArgs {
@@ -117,6 +120,9 @@ struct ResolveArgs {
 
 // launchers (all asynchronous on `stream`)
 void launch_block_cull(const BlockView& b, const FrameConst& fc, const HizView& hiz, cudaStream_t stream);
+// Lists the 32-Gaussian chunks that hold at least one unculled block and zeroes the survivor
+// mask words of the others.
+void launch_visible_chunks(const BlockView& b, uint32_t n, uint32_t* list, uint32_t* mask_cur, cudaStream_t stream);
 void launch_preprocess_fp32(const PreprocessArgs& a, const SceneFP32& s, cudaStream_t stream);
 void launch_preprocess_compressed(const PreprocessArgs& a, const SceneCompressed& s, cudaStream_t stream);
 void launch_scan(const ScanArgs& a, uint32_t scan_tiles, cudaStream_t stream);

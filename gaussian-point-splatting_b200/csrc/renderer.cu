@@ -221,7 +221,7 @@ struct gps_renderer {
     uint64_t entries = 0;
     uint32_t n = 0, n_pad = 0;
     dptr<uint64_t> buffer;
-    dptr<uint32_t> counts, mask[2], surv_gid, surv_start, tile_first_rank, ticket, culled;
+    dptr<uint32_t> counts, mask[2], surv_gid, surv_start, tile_first_rank, ticket, culled, chunk_list, chunk_count;
     dptr<SplatRecord> records;
     dptr<unsigned long long> tile_state;
     dptr<PassCounters> counters;  // [2]: pass 1, pass 2
@@ -299,6 +299,7 @@ BlockView block_view(gps_renderer* r) {
     BlockView b{};
     b.nodes = r->scene->block_nodes.get();
     b.culled = r->culled.get();
+    b.chunk_count = r->chunk_count.get();
     b.node_count = r->scene->block_count;
     b.words = (b.node_count + 31) / 32;
     b.per_block = r->scene->per_block;
@@ -313,10 +314,13 @@ void count_launch(gps_renderer* r, int stage, uint64_t n = 1) {
 void render_pass(gps_renderer* r, const FrameConst& fc, int frame, bool first, cudaStream_t st) {
     const int frame_seed = 4 * frame + (first ? 0 : 2);
     BlockView blocks = block_view(r);
-    if (fc.enable_hier && blocks.node_count) {
+    const bool listed = fc.enable_hier && blocks.node_count;
+    uint32_t* mask_cur = r->mask[r->iteration % 2].get();
+    if (listed) {
         r->timer.mark(kStCull, st);
         launch_block_cull(blocks, fc, r->hiz, st);
-        count_launch(r, kStCull);
+        launch_visible_chunks(blocks, r->n, r->chunk_list.get(), mask_cur, st);
+        count_launch(r, kStCull, 2);
     }
     r->timer.mark(kStPreprocess, st);
     PreprocessArgs pa{};
@@ -330,6 +334,8 @@ void render_pass(gps_renderer* r, const FrameConst& fc, int frame, bool first, c
     pa.records = r->records.get();
     pa.hiz = r->hiz;
     pa.blocks = blocks;
+    pa.chunk_list = listed ? r->chunk_list.get() : nullptr;
+    pa.chunk_count = listed ? r->chunk_count.get() : nullptr;
     if (r->scene->format == GPS_SCENE_FP32) {
         SceneFP32 s{r->scene->pos_op.get(), r->scene->rot.get(), r->scene->scale.get(), r->scene->sh.get(), r->n};
         launch_preprocess_fp32(pa, s, st);
@@ -587,6 +593,9 @@ gps_status gps_renderer_create(gps_scene* scene, const gps_settings* settings, g
         GPS_CUDA(cudaMemset(r->counters.get(), 0, sizeof(PassCounters) * 2));
         const uint32_t bwords = (scene->block_count + 31) / 32;
         r->culled.reset(dev_alloc<uint32_t>(bwords + 1));
+        r->chunk_list.reset(dev_alloc<uint32_t>(words + 1));
+        r->chunk_count.reset(dev_alloc<uint32_t>(1));
+        GPS_CUDA(cudaMemset(r->chunk_count.get(), 0, sizeof(uint32_t)));
         GPS_CUDA(cudaMemset(r->culled.get(), 0, sizeof(uint32_t) * (bwords + 1)));
         hiz_layout(r->hiz, s.width, s.height);
         r->mip.reset(dev_alloc<float>(r->hiz.mip_size));

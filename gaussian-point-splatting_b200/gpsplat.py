@@ -16,7 +16,8 @@ from ctypes import POINTER, byref, c_char, c_char_p, c_float, c_int32, c_uint8, 
 import numpy as np
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_HERE, "libgps_b200.so")
+# GPS_B200_LIBRARY points at a libgps_b200.so built elsewhere (e.g. with other tuning options)
+LIB_PATH = os.environ.get("GPS_B200_LIBRARY") or os.path.join(_HERE, "libgps_b200.so")
 
 GPS_SCENE_FP32 = 0
 GPS_SCENE_COMPRESSED = 1
