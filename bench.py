@@ -232,6 +232,120 @@ def run_reference_arm(args, spec, world, rank):
 
 
 # ---------------------------------------------------------------------------------
+# batched multi-view workload: 64 views of the 16M town, views/s batch vs plain
+# ---------------------------------------------------------------------------------
+BATCH_RES = [(320, 180), (640, 360), (1280, 720), (1920, 1080)]
+BATCH_SPP = [1, 2, 4, 8, 16]
+
+
+def run_batch_workload(args, world, rank, local):
+    """One step = one batch of 64 views (seeded random poses inside the town, resolution and
+    spp drawn from BATCH_RES x BATCH_SPP, supersampling 2, BVH + Hi-Z culling) rendered by
+    gps_batch_render; the same 64 views rendered one at a time through gps_renderer_reset +
+    gps_render_frame (one renderer per view configuration, one stream) is the plain path timed
+    beside it, and the two must agree bit for bit."""
+    import torch
+
+    torch.cuda.set_device(local)
+    import gpsplat
+
+    gpsplat.load_library()
+    spec = workload_spec("town16m")
+    g_host = load_scene_host(spec)
+    scene = gpsplat.Scene.from_host(np.ascontiguousarray(g_host), presorted=True)
+    base = dict(supersampling_factor=2, enable_hierarchical_culling=1, enable_occlusion_culling=1)
+    rng = np.random.default_rng(64 + rank)
+    poses = synth.random_poses(64, seed=7 + rank)
+    views = []
+    for i, (p, r) in enumerate(poses):
+        w, h = BATCH_RES[int(rng.integers(len(BATCH_RES)))]
+        spp = BATCH_SPP[int(rng.integers(len(BATCH_SPP)))]
+        s = gpsplat.default_settings(**base, width=w, height=h, samples_per_pixel=spp)
+        cam = gpsplat.camera_from_pose(p, np.asarray(r, np.float32).T, s, i + 1)
+        views.append(dict(cam=cam, w=w, h=h, spp=spp, s=s, img=torch.empty((h, w, 3), device="cuda"),
+                          dep=torch.empty((h, w), device="cuda"), pimg=torch.empty((h, w, 3), device="cuda"),
+                          pdep=torch.empty((h, w), device="cuda")))
+    arr = gpsplat.Batch.views([(v["cam"], v["w"], v["h"], v["spp"], v["img"].data_ptr(), v["dep"].data_ptr()) for v in views])
+    cap = gpsplat.default_settings(**base, width=1920, height=1080, samples_per_pixel=16)
+    batch = gpsplat.Batch(scene, cap, 1920, 1080, 16, workers=8)
+    stream = torch.cuda.Stream()
+    sh = stream.cuda_stream
+    chosen, tune_ms = batch.autotune(arr, rounds=1, stream=sh)
+    renderers = {}
+    for v in views:
+        key = (v["w"], v["h"], v["spp"])
+        if key not in renderers:
+            renderers[key] = gpsplat.Renderer(scene, v["s"])
+
+    def plain_round():
+        for v in views:  # each view as a fresh single-view render, like the batch's
+            r = renderers[(v["w"], v["h"], v["spp"])]
+            r.reset(sh)
+            r.render(v["cam"], v["pimg"].data_ptr(), v["pdep"].data_ptr(), sh)
+
+    for _ in range(args.warmup):
+        batch.render(arr, sh)
+        plain_round()
+    torch.cuda.synchronize()
+    same = all(torch.equal(v["img"].view(torch.int32), v["pimg"].view(torch.int32)) and
+               torch.equal(v["dep"].view(torch.int32), v["pdep"].view(torch.int32)) for v in views)
+
+    def timed(fn):
+        barrier(world)
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return max_over_ranks(e0.elapsed_time(e1), world)
+
+    sampler = ClockSampler(local)
+    sampler.start()
+    time.sleep(0.3)
+    batch_ms = timed(lambda: batch.render(arr, sh))
+    clocks = sampler.stop()
+    plain_ms = timed(plain_round)
+    # end to end: every view's image read back to pinned host memory each step
+    host = [torch.empty((v["h"], v["w"], 3), dtype=torch.float32, pin_memory=True) for v in views]
+
+    def e2e_step():
+        batch.render(arr, sh)
+        for v, hb in zip(views, host):
+            hb.copy_(v["img"], non_blocking=True)
+
+    with torch.cuda.stream(stream):
+        e2e_ms = timed(e2e_step)
+    d2h = sum(v["w"] * v["h"] * 12 for v in views)
+    n_views = len(views) * args.steps * world
+    value = n_views / (batch_ms / 1000.0)
+    line = {
+        "metric": "views/sec", "value": value, "unit": "views/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": batch_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded town and poses, see synth.py)",
+        "config": {"workload": "batch64", "gaussians": scene.count, "views_per_step": len(views),
+                   "resolutions": BATCH_RES, "spp": BATCH_SPP, "supersampling": 2, "culling": True,
+                   "l2": "inputs larger than L2 (scene 3.8 GB)", "parallelism": f"replicas x{world}"},
+        "plain": {"value": n_views / (plain_ms / 1000.0), "unit": "views/s", "ms_per_step": plain_ms / args.steps},
+        "speedup_vs_plain": plain_ms / batch_ms,
+        "bit_exact_vs_plain": bool(same),
+        "autotune": {"workers": chosen, "ms_per_batch": tune_ms},
+        "clocks": clocks,
+        "e2e": {"value": n_views / (e2e_ms / 1000.0), "unit": "views/s", "h2d_bytes_per_step": len(bytes(arr)),
+                "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms / args.steps},
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    batch.close()
+    for r in renderers.values():
+        r.close()
+    scene.close()
+    return 0
+
+
+# ---------------------------------------------------------------------------------
 # the GPU arm
 # ---------------------------------------------------------------------------------
 def main():
@@ -240,12 +354,19 @@ def main():
     ap.add_argument("--steps", type=int, default=30)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="mine", choices=["mine", "reference"])
-    ap.add_argument("--workload", default="town16m", choices=["town16m", "town4m", "cube1m"])
+    ap.add_argument("--workload", default="town16m", choices=["town16m", "town4m", "cube1m", "batch64"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
-    spec = workload_spec(args.workload)
     world, rank, local = dist_init()
+    if args.workload == "batch64":
+        if args.impl == "reference":
+            if rank == 0:
+                print(json.dumps({"impl": "reference", "unavailable": "the reference renders one view per call; the "
+                                  "batch64 views/s comparison is against this library's plain single-view path"}))
+            return 0
+        return run_batch_workload(args, world, rank, local)
+    spec = workload_spec(args.workload)
     if args.impl == "reference":
         return run_reference_arm(args, spec, world, rank)
 

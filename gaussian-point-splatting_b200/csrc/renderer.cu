@@ -7,6 +7,7 @@
 // Unlike the reference it performs no host synchronisation and no allocation per frame:
 // the point count P stays on the device (the splat kernel reads it), so the whole frame is
 // a fixed sequence of asynchronous launches on the caller's stream.
+#include <algorithm>
 #include <cstdio>
 #include <cstring>
 #include <memory>
@@ -229,6 +230,8 @@ struct gps_renderer {
     dptr<unsigned> hiz_done;
     HizView hiz{};
     uint32_t scan_tiles = 0;
+    uint64_t cap_entries = 0;     // splat-buffer and Hi-Z capacity (a batch worker renders
+    uint64_t cap_mip = 0;         // views of different sizes within these)
     uint32_t iteration = 0;
     int splat_grid = 0;
     PassCounters* host_counters = nullptr;  // pinned [2]
@@ -552,10 +555,54 @@ gps_status gps_ply_read(const char* path, float* out, uint64_t capacity, uint64_
     return GPS_OK;
 }
 
-gps_status gps_renderer_create(gps_scene* scene, const gps_settings* settings, gps_renderer** out) {
-    if (!scene || !settings || !out) return fail(GPS_ERR_INVALID_ARGUMENT, "null argument");
+}  // extern "C"
+
+namespace {
+
+gps_status check_view_size(const gps_settings& s, uint64_t* entries_out) {
+    if (s.width <= 0 || s.height <= 0 || s.supersampling_factor <= 0 || s.samples_per_pixel <= 0)
+        return fail(GPS_ERR_INVALID_ARGUMENT, "resolution, supersampling factor and samples per pixel must be positive");
+    const uint64_t up_w = (uint64_t)s.width * s.supersampling_factor, up_h = (uint64_t)s.height * s.supersampling_factor;
+    if (up_w > 65504 || up_h > 65504) return fail(GPS_ERR_SIZE, "supersampled resolution above 65504 pixels per axis");
+    const uint64_t entries = splat_buffer_entries((int)up_w, (int)up_h, s.samples_per_pixel);
+    if (entries >= (1ull << 31)) return fail(GPS_ERR_SIZE, "splat buffer above 2^31 entries");
+    *entries_out = entries;
+    return GPS_OK;
+}
+
+// Makes r render width x height at spp samples per pixel from now on, within its capacity.
+gps_status configure_view(gps_renderer* r, int32_t width, int32_t height, int32_t spp) {
+    gps_settings s = r->s;
+    s.width = width;
+    s.height = height;
+    s.samples_per_pixel = spp;
+    uint64_t entries = 0;
+    gps_status st = check_view_size(s, &entries);
+    if (st != GPS_OK) return st;
+    HizView h = r->hiz;
+    hiz_layout(h, width, height);
+    if (entries > r->cap_entries || h.mip_size > r->cap_mip)
+        return fail(GPS_ERR_SIZE, "view of " + std::to_string(width) + "x" + std::to_string(height) + " at " +
+                                      std::to_string(spp) + " spp exceeds the renderer's capacity");
+    r->s = s;
+    r->up_w = width * s.supersampling_factor;
+    r->up_h = height * s.supersampling_factor;
+    r->entries = entries;
+    r->hiz = h;
+    return GPS_OK;
+}
+
+// A renderer for `settings` whose splat buffer and Hi-Z also fit views of `capacity`'s size.
+gps_status create_renderer(gps_scene* scene, const gps_settings* settings, const gps_settings* capacity,
+                           gps_renderer** out) {
+    if (!scene || !settings || !capacity || !out) return fail(GPS_ERR_INVALID_ARGUMENT, "null argument");
     *out = nullptr;
     const gps_settings& s = *settings;
+    uint64_t cap_entries = 0;
+    const gps_status cs = check_view_size(*capacity, &cap_entries);
+    if (cs != GPS_OK) return cs;
+    HizView cap_hiz{};
+    hiz_layout(cap_hiz, capacity->width, capacity->height);
     if (s.width <= 0 || s.height <= 0 || s.supersampling_factor <= 0 || s.samples_per_pixel <= 0)
         return fail(GPS_ERR_INVALID_ARGUMENT, "resolution, supersampling factor and samples per pixel must be positive");
     if (!(s.far_view_plane > s.near_view_plane) || !(s.fovy > 0.0f))
@@ -573,8 +620,9 @@ gps_status gps_renderer_create(gps_scene* scene, const gps_settings* settings, g
     r->n = (uint32_t)scene->n;
     r->scan_tiles = scan_tile_count(r->n);
     r->n_pad = r->scan_tiles * 4096;
+    r->cap_entries = std::max(entries, cap_entries);
     try {
-        r->buffer.reset(dev_alloc<uint64_t>(entries));
+        r->buffer.reset(dev_alloc<uint64_t>(r->cap_entries));
         r->counts.reset(dev_alloc<uint32_t>(std::max<uint32_t>(r->n_pad, 16)));
         GPS_CUDA(cudaMemset(r->counts.get(), 0, sizeof(uint32_t) * std::max<uint32_t>(r->n_pad, 16)));
         const uint32_t words = (r->n + 31) / 32;
@@ -598,14 +646,15 @@ gps_status gps_renderer_create(gps_scene* scene, const gps_settings* settings, g
         GPS_CUDA(cudaMemset(r->chunk_count.get(), 0, sizeof(uint32_t)));
         GPS_CUDA(cudaMemset(r->culled.get(), 0, sizeof(uint32_t) * (bwords + 1)));
         hiz_layout(r->hiz, s.width, s.height);
-        r->mip.reset(dev_alloc<float>(r->hiz.mip_size));
+        r->cap_mip = std::max(r->hiz.mip_size, cap_hiz.mip_size);
+        r->mip.reset(dev_alloc<float>(r->cap_mip));
         r->hiz.mip = r->mip.get();
         r->hiz_done.reset(dev_alloc<unsigned>(1));
         GPS_CUDA(cudaMemset(r->hiz_done.get(), 0, sizeof(unsigned)));
         r->hiz.done = r->hiz_done.get();
         // the reference leaves its Hi-Z uninitialised before the first frame; +inf here
         // means "nothing occluded" for frame 1
-        fill_f32<<<148 * 4, 256>>>(r->mip.get(), r->hiz.mip_size, INFINITY);
+        fill_f32<<<148 * 4, 256>>>(r->mip.get(), r->cap_mip, INFINITY);
         GPS_CUDA(cudaGetLastError());
         GPS_CUDA(cudaMallocHost(&r->host_counters, sizeof(PassCounters) * 2));
         std::memset(r->host_counters, 0, sizeof(PassCounters) * 2);
@@ -619,6 +668,16 @@ gps_status gps_renderer_create(gps_scene* scene, const gps_settings* settings, g
     return GPS_OK;
 }
 
+gps_status render_frame_impl(gps_renderer* r, const gps_camera* cam, float* d_image, float* d_depth, cudaStream_t st);
+
+}  // namespace
+
+extern "C" {
+
+gps_status gps_renderer_create(gps_scene* scene, const gps_settings* settings, gps_renderer** out) {
+    return create_renderer(scene, settings, settings, out);
+}
+
 void gps_renderer_free(gps_renderer* r) {
     if (r) cudaDeviceSynchronize();
     delete r;
@@ -626,7 +685,13 @@ void gps_renderer_free(gps_renderer* r) {
 
 gps_status gps_render_frame(gps_renderer* r, const gps_camera* cam, float* d_image, float* d_depth, void* stream) {
     if (!r || !cam || !d_image || !d_depth) return fail(GPS_ERR_INVALID_ARGUMENT, "null argument");
-    cudaStream_t st = as_stream(stream);
+    return render_frame_impl(r, cam, d_image, d_depth, as_stream(stream));
+}
+
+}  // extern "C"
+
+namespace {
+gps_status render_frame_impl(gps_renderer* r, const gps_camera* cam, float* d_image, float* d_depth, cudaStream_t st) {
     const FrameConst fc = make_frame_const(r, cam);
     const uint64_t bg = 0xFFFFFFF000000000ull |
                         rgb_to_36bits(make_v3(r->s.background[0], r->s.background[1], r->s.background[2]));
@@ -677,6 +742,17 @@ gps_status gps_render_frame(gps_renderer* r, const gps_camera* cam, float* d_ima
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return fail(GPS_ERR_CUDA, std::string("frame launch failed: ") + cudaGetErrorString(e));
     return GPS_OK;
+}
+}  // namespace
+
+extern "C" {
+
+gps_status gps_renderer_reset(gps_renderer* r, void* stream) {
+    if (!r) return fail(GPS_ERR_INVALID_ARGUMENT, "null argument");
+    fill_f32<<<148, 256, 0, as_stream(stream)>>>(r->mip.get(), r->hiz.mip_size, INFINITY);
+    r->iteration = 0;
+    cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? GPS_OK : fail(GPS_ERR_CUDA, cudaGetErrorString(e));
 }
 
 gps_status gps_renderer_stats(gps_renderer* r, gps_stats* out) {
@@ -799,6 +875,153 @@ gps_status gps_post_progressive(uint8_t* d_image_u8, float* d_cur_color, float* 
     launch_progressive(d_image_u8, d_cur_color, d_accum, width, height, frames, as_stream(stream));
     cudaError_t e = cudaGetLastError();
     return e == cudaSuccess ? GPS_OK : fail(GPS_ERR_CUDA, cudaGetErrorString(e));
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------------
+// batched multi-view rendering
+// ---------------------------------------------------------------------------------
+struct gps_batch {
+    gps_settings s{};
+    std::vector<gps_renderer*> workers;
+    std::vector<cudaStream_t> streams;
+    std::vector<cudaEvent_t> joined;
+    cudaEvent_t forked = nullptr;
+    int active = 1;
+    ~gps_batch() {
+        cudaDeviceSynchronize();
+        for (gps_renderer* w : workers) delete w;
+        for (cudaStream_t st : streams) cudaStreamDestroy(st);
+        for (cudaEvent_t e : joined) cudaEventDestroy(e);
+        if (forked) cudaEventDestroy(forked);
+    }
+};
+
+namespace {
+
+// Renders one view on worker w as a fresh renderer's first frame would.
+gps_status render_view(gps_renderer* w, const gps_view& v, cudaStream_t st) {
+    gps_status rc = configure_view(w, v.width, v.height, v.samples_per_pixel);
+    if (rc != GPS_OK) return rc;
+    if (w->s.enable_occlusion_culling) fill_f32<<<148, 256, 0, st>>>(w->mip.get(), w->hiz.mip_size, INFINITY);
+    w->iteration = 0;
+    return render_frame_impl(w, &v.camera, v.d_image, v.d_depth, st);
+}
+
+// Longest-processing-time-first assignment of views to workers by estimated cost (buffer
+// entries cleared and resolved, plus a per-view share for the culling and preprocess).
+std::vector<int> assign_views(const gps_batch* b, const gps_view* views, int32_t count, uint64_t n_gaussians) {
+    std::vector<std::pair<double, int>> cost(count);
+    const double ss = b->s.supersampling_factor;
+    for (int i = 0; i < count; ++i)
+        cost[i] = {(double)views[i].width * views[i].height * ss * ss * views[i].samples_per_pixel + 0.05 * (double)n_gaussians, i};
+    std::sort(cost.begin(), cost.end(), [](const auto& x, const auto& y) { return x.first > y.first; });
+    std::vector<double> load(b->active, 0.0);
+    std::vector<int> owner(count, 0);
+    for (const auto& c : cost) {
+        const int w = (int)(std::min_element(load.begin(), load.end()) - load.begin());
+        owner[c.second] = w;
+        load[w] += c.first;
+    }
+    return owner;
+}
+
+}  // namespace
+
+extern "C" {
+
+gps_status gps_batch_create(gps_scene* scene, const gps_settings* settings, int32_t max_width, int32_t max_height,
+                            int32_t max_spp, int32_t workers, gps_batch** out) {
+    if (!scene || !settings || !out) return fail(GPS_ERR_INVALID_ARGUMENT, "null argument");
+    *out = nullptr;
+    if (workers < 1 || workers > 64) return fail(GPS_ERR_INVALID_ARGUMENT, "workers must be 1..64");
+    auto b = std::make_unique<gps_batch>();
+    b->s = *settings;
+    gps_settings cap = *settings;
+    cap.width = max_width;
+    cap.height = max_height;
+    cap.samples_per_pixel = max_spp;
+    for (int i = 0; i < workers; ++i) {
+        gps_renderer* w = nullptr;
+        gps_status rc = create_renderer(scene, &cap, &cap, &w);
+        if (rc != GPS_OK) return rc;
+        b->workers.push_back(w);
+        cudaStream_t st = nullptr;
+        cudaEvent_t e = nullptr;
+        if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess ||
+            cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess)
+            return fail(GPS_ERR_CUDA, "stream or event creation failed");
+        b->streams.push_back(st);
+        b->joined.push_back(e);
+    }
+    if (cudaEventCreateWithFlags(&b->forked, cudaEventDisableTiming) != cudaSuccess)
+        return fail(GPS_ERR_CUDA, "event creation failed");
+    b->active = workers;
+    *out = b.release();
+    return GPS_OK;
+}
+
+void gps_batch_free(gps_batch* b) { delete b; }
+
+gps_status gps_batch_set_workers(gps_batch* b, int32_t workers) {
+    if (!b || workers < 1 || workers > (int32_t)b->workers.size()) return fail(GPS_ERR_INVALID_ARGUMENT, "bad worker count");
+    b->active = workers;
+    return GPS_OK;
+}
+
+int32_t gps_batch_workers(const gps_batch* b) { return b ? b->active : 0; }
+
+gps_status gps_batch_render(gps_batch* b, const gps_view* views, int32_t count, void* stream) {
+    if (!b || (count > 0 && !views) || count < 0) return fail(GPS_ERR_INVALID_ARGUMENT, "null argument");
+    for (int i = 0; i < count; ++i)
+        if (!views[i].d_image || !views[i].d_depth) return fail(GPS_ERR_INVALID_ARGUMENT, "view without output buffers");
+    cudaStream_t st = as_stream(stream);
+    const std::vector<int> owner = assign_views(b, views, count, b->workers[0]->n);
+    cudaEventRecord(b->forked, st);
+    for (int w = 0; w < b->active; ++w) cudaStreamWaitEvent(b->streams[w], b->forked, 0);
+    gps_status rc = GPS_OK;
+    for (int i = 0; i < count && rc == GPS_OK; ++i) rc = render_view(b->workers[owner[i]], views[i], b->streams[owner[i]]);
+    for (int w = 0; w < b->active; ++w) {
+        cudaEventRecord(b->joined[w], b->streams[w]);
+        cudaStreamWaitEvent(st, b->joined[w], 0);
+    }
+    if (rc != GPS_OK) return rc;
+    cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? GPS_OK : fail(GPS_ERR_CUDA, std::string("batch launch failed: ") + cudaGetErrorString(e));
+}
+
+gps_status gps_batch_autotune(gps_batch* b, const gps_view* views, int32_t count, int32_t rounds, void* stream,
+                              int32_t* chosen, float* ms) {
+    if (!b || rounds < 1) return fail(GPS_ERR_INVALID_ARGUMENT, "bad argument");
+    cudaStream_t st = as_stream(stream);
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    int best = 1;
+    float best_ms = 0.0f;
+    gps_status rc = GPS_OK;
+    for (int w = 1; w <= (int)b->workers.size() && rc == GPS_OK; w *= 2) {
+        b->active = w;
+        rc = gps_batch_render(b, views, count, stream);  // warm-up at this width
+        cudaEventRecord(e0, st);
+        for (int r = 0; r < rounds && rc == GPS_OK; ++r) rc = gps_batch_render(b, views, count, stream);
+        cudaEventRecord(e1, st);
+        cudaEventSynchronize(e1);
+        float t = 0.0f;
+        cudaEventElapsedTime(&t, e0, e1);
+        t /= (float)rounds;
+        if (w == 1 || t < best_ms) {
+            best = w;
+            best_ms = t;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    b->active = best;
+    if (chosen) *chosen = best;
+    if (ms) *ms = best_ms;
+    return rc;
 }
 
 }  // extern "C"

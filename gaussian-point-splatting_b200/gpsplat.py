@@ -81,6 +81,12 @@ class Camera(ctypes.Structure):
     ]
 
 
+class View(ctypes.Structure):
+    """gps_view: one view of a batch."""
+    _fields_ = [("camera", Camera), ("width", c_int32), ("height", c_int32), ("samples_per_pixel", c_int32),
+                ("d_image", c_void_p), ("d_depth", c_void_p)]
+
+
 class CameraState(ctypes.Structure):
     _fields_ = [
         ("id", c_int32),
@@ -146,6 +152,7 @@ _SIGNATURES = [
     ("gps_renderer_create", c_int32, [c_void_p, POINTER(Settings), POINTER(c_void_p)]),
     ("gps_renderer_free", None, [c_void_p]),
     ("gps_render_frame", c_int32, [c_void_p, POINTER(Camera), c_void_p, c_void_p, c_void_p]),
+    ("gps_renderer_reset", c_int32, [c_void_p, c_void_p]),
     ("gps_renderer_stats", c_int32, [c_void_p, POINTER(Stats)]),
     ("gps_renderer_enable_timing", c_int32, [c_void_p, c_int32]),
     ("gps_renderer_stage_times", c_int32, [c_void_p, POINTER(c_float), POINTER(c_uint64), c_int32]),
@@ -155,6 +162,12 @@ _SIGNATURES = [
     ("gps_post_taa", c_int32, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, POINTER(c_float), c_float, c_int32, c_int32, c_int32, c_void_p]),
     ("gps_post_progressive", c_int32, [c_void_p, c_void_p, c_void_p, c_int32, c_int32, c_int32, c_void_p]),
     ("gps_workload_scan_noalloc", c_int32, [c_void_p, c_void_p, c_uint32, c_uint32, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
+    ("gps_batch_create", c_int32, [c_void_p, POINTER(Settings), c_int32, c_int32, c_int32, c_int32, POINTER(c_void_p)]),
+    ("gps_batch_free", None, [c_void_p]),
+    ("gps_batch_render", c_int32, [c_void_p, POINTER(View), c_int32, c_void_p]),
+    ("gps_batch_set_workers", c_int32, [c_void_p, c_int32]),
+    ("gps_batch_workers", c_int32, [c_void_p]),
+    ("gps_batch_autotune", c_int32, [c_void_p, POINTER(View), c_int32, c_int32, c_void_p, POINTER(c_int32), POINTER(c_float)]),
     ("gps_frame_loop_create", c_int32, [c_void_p, POINTER(c_void_p)]),
     ("gps_frame_loop_free", None, [c_void_p]),
     ("gps_frame_loop_step", c_int32, [c_void_p, POINTER(Camera), c_void_p]),
@@ -348,6 +361,10 @@ class Renderer:
         """RenderPass::render into caller-owned device buffers (raw device pointers)."""
         _check(load_library().gps_render_frame(self._h, byref(cam), c_void_p(d_image), c_void_p(d_depth), c_void_p(stream)))
 
+    def reset(self, stream: int = 0):
+        """Forget the previous frame: the next render is that of a fresh renderer."""
+        _check(load_library().gps_renderer_reset(self._h, c_void_p(stream)))
+
     def stats(self) -> Stats:
         st = Stats()
         _check(load_library().gps_renderer_stats(self._h, byref(st)))
@@ -383,6 +400,54 @@ class Renderer:
     def close(self):
         if self._h:
             load_library().gps_renderer_free(self._h)
+            self._h = c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Batch:
+    """Many views of one scene per call (gps_batch_*): each view bit-identical to a fresh
+    single-view render, the views spread over `workers` streams."""
+
+    def __init__(self, scene: Scene, settings: Settings, max_width: int, max_height: int, max_spp: int, workers: int = 4):
+        self.scene = scene
+        self._h = c_void_p()
+        _check(load_library().gps_batch_create(scene._h, byref(settings), max_width, max_height, max_spp, workers,
+                                               byref(self._h)))
+
+    @staticmethod
+    def views(entries) -> "ctypes.Array":
+        """entries: (Camera, width, height, spp, d_image, d_depth) tuples -> gps_view array."""
+        arr = (View * len(entries))()
+        for i, (cam, w, h, spp, img, dep) in enumerate(entries):
+            arr[i] = View(cam, w, h, spp, c_void_p(img), c_void_p(dep))
+        return arr
+
+    def render(self, views, stream: int = 0):
+        _check(load_library().gps_batch_render(self._h, views, len(views), c_void_p(stream)))
+
+    @property
+    def workers(self) -> int:
+        return load_library().gps_batch_workers(self._h)
+
+    @workers.setter
+    def workers(self, n: int):
+        _check(load_library().gps_batch_set_workers(self._h, n))
+
+    def autotune(self, views, rounds: int = 2, stream: int = 0):
+        chosen = c_int32()
+        ms = c_float()
+        _check(load_library().gps_batch_autotune(self._h, views, len(views), rounds, c_void_p(stream), byref(chosen),
+                                                 byref(ms)))
+        return chosen.value, ms.value
+
+    def close(self):
+        if self._h:
+            load_library().gps_batch_free(self._h)
             self._h = c_void_p()
 
     def __del__(self):

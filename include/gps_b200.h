@@ -144,6 +144,10 @@ void gps_renderer_free(gps_renderer* r);
  * device buffers).  No host synchronisation and no allocation inside. */
 gps_status gps_render_frame(gps_renderer* r, const gps_camera* cam, float* d_image_rgb, float* d_depth,
                             void* stream);
+/* Forgets the previous frame (its Hi-Z depth chain): the next gps_render_frame renders as the
+ * first frame of a newly created renderer would, e.g. after a camera cut.  Asynchronous on
+ * `stream`. */
+gps_status gps_renderer_reset(gps_renderer* r, void* stream);
 /* Statistics of the last frame; waits for that frame's work on its stream. */
 gps_status gps_renderer_stats(gps_renderer* r, gps_stats* out);
 /* Per-stage GPU timing with CUDA events on the frame's stream (off by default).  Stages:
@@ -202,6 +206,38 @@ gps_status gps_renderer_debug_view(gps_renderer* r, gps_debug_view* out);
 gps_status gps_workload_scan_noalloc(const uint32_t* d_counts, const uint32_t* d_mask, uint32_t n,
                                      uint32_t max_points, uint32_t* d_surv_gid, uint32_t* d_surv_start,
                                      uint32_t* d_tile_first_rank, uint32_t* d_counters8, void* stream);
+
+/* ---- batched multi-view rendering ----------------------------------------------------
+ * Many views of one scene per call, each with its own camera, resolution and samples per
+ * pixel, written to caller-owned device buffers.  Each view is rendered as the first frame of
+ * a fresh gps_render_frame renderer would render it (no temporal Hi-Z reuse), so its image and
+ * depth are bit-identical to that plain render.  Views run on `workers` internal streams that
+ * fork from and join back into `stream`, so views too small to fill the GPU overlap.  Workers
+ * hold per-Gaussian scratch sized for the scene and a splat buffer sized for the largest view
+ * (max_width x max_height at max_spp); views beyond that capacity return GPS_ERR_SIZE.  The
+ * other fields of `settings` (supersampling, culling, K mode, planes, fovy, background) apply to
+ * every view. */
+typedef struct gps_view {
+    gps_camera camera;
+    int32_t width, height;       /* output resolution of this view */
+    int32_t samples_per_pixel;
+    float* d_image;              /* width * height float3 (device) */
+    float* d_depth;              /* width * height float NDC depth (device) */
+} gps_view;
+typedef struct gps_batch gps_batch;
+gps_status gps_batch_create(gps_scene* scene, const gps_settings* settings, int32_t max_width, int32_t max_height,
+                            int32_t max_spp, int32_t workers, gps_batch** out);
+void gps_batch_free(gps_batch* b);
+/* Enqueues every view; returns without waiting for the GPU. */
+gps_status gps_batch_render(gps_batch* b, const gps_view* views, int32_t count, void* stream);
+/* Number of workers used by gps_batch_render (1 .. the number created). */
+gps_status gps_batch_set_workers(gps_batch* b, int32_t workers);
+int32_t gps_batch_workers(const gps_batch* b);
+/* Autotuner: times `rounds` renders of the batch for each worker count 1, 2, 4, ... up to the
+ * number created (CUDA events on `stream`), keeps the fastest and returns it in *chosen and its
+ * time per batch in *ms (either may be NULL).  Synchronises `stream`. */
+gps_status gps_batch_autotune(gps_batch* b, const gps_view* views, int32_t count, int32_t rounds, void* stream,
+                              int32_t* chosen, float* ms);
 
 /* ---- RenderServer post-process (render_server.cu:122-157) ---------------------------- */
 /* temporalRender (post_processing_kernels.cuh:222-285): reprojects history through reproj

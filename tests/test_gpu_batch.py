@@ -1,0 +1,109 @@
+"""Batched multi-view rendering (gps_batch_*) against plain single-view renders.
+
+A batch renders every view as a fresh renderer's first frame, so each view's image and depth
+must be bit-identical to gps_render_frame on a renderer created for that view alone, whatever
+the mix of resolutions and samples per pixel, the number of workers or the order of views.
+"""
+import numpy as np
+import pytest
+
+import gpsplat
+import gpsutil
+import synth
+
+pytestmark = pytest.mark.gpu
+
+RES = [(320, 180), (640, 360), (160, 90), (400, 240)]
+SPP = [1, 2, 4, 8]
+
+
+def _views(n, seed):
+    rng = np.random.default_rng(seed)
+    poses = synth.random_poses(n, seed=seed)
+    out = []
+    for i in range(n):
+        w, h = RES[int(rng.integers(len(RES)))]
+        spp = SPP[int(rng.integers(len(SPP)))]
+        out.append((poses[i], w, h, spp, 1 + int(rng.integers(50))))
+    return out
+
+
+def _plain(scene, base, view):
+    import torch
+
+    (pose, w, h, spp, frame) = view
+    s = gpsplat.default_settings(**base, width=w, height=h, samples_per_pixel=spp)
+    cam = gpsutil.cameras_for(s, [pose], first_frame=frame)[0]
+    r = gpsplat.Renderer(scene, s)
+    img = torch.empty((h, w, 3), dtype=torch.float32, device="cuda")
+    dep = torch.empty((h, w), dtype=torch.float32, device="cuda")
+    r.render(cam, img.data_ptr(), dep.data_ptr(), 0)
+    torch.cuda.synchronize()
+    r.close()
+    return cam, img.cpu().numpy(), dep.cpu().numpy()
+
+
+@pytest.mark.parametrize("occlusion,workers", [(1, 4), (0, 3)])
+def test_batch_matches_plain_renders(occlusion, workers):
+    import torch
+
+    ply = gpsutil.cached_ply("town60k", lambda: synth.town(60000, seed=5))
+    scene = gpsplat.Scene.from_ply(ply)
+    base = dict(supersampling_factor=2, enable_occlusion_culling=occlusion, max_number_of_points=4_000_000)
+    views = _views(10, seed=11 + occlusion)
+    plain = [_plain(scene, base, v) for v in views]
+    s = gpsplat.default_settings(**base, width=640, height=360, samples_per_pixel=8)
+    batch = gpsplat.Batch(scene, s, 640, 360, 8, workers=workers)
+    bufs = [(torch.full((v[2], v[1], 3), -1.0, device="cuda"), torch.full((v[2], v[1]), -1.0, device="cuda")) for v in views]
+    entries = [(plain[i][0], v[1], v[2], v[3], bufs[i][0].data_ptr(), bufs[i][1].data_ptr()) for i, v in enumerate(views)]
+    arr = gpsplat.Batch.views(entries)
+    for call in range(2):  # twice: worker state left by one batch must not leak into the next
+        batch.render(arr)
+        torch.cuda.synchronize()
+        for i in range(len(views)):
+            img, dep = bufs[i][0].cpu().numpy(), bufs[i][1].cpu().numpy()
+            assert np.array_equal(img.view(np.uint32), plain[i][1].view(np.uint32)), f"call {call} view {i}: image differs"
+            assert np.array_equal(dep.view(np.uint32), plain[i][2].view(np.uint32)), f"call {call} view {i}: depth differs"
+    chosen, ms = batch.autotune(arr, rounds=1)
+    assert 1 <= chosen <= workers and ms > 0
+    batch.close()
+    scene.close()
+
+
+def test_batch_rejects_views_beyond_capacity():
+    import torch
+
+    ply = gpsutil.cached_ply("town60k", lambda: synth.town(60000, seed=5))
+    scene = gpsplat.Scene.from_ply(ply)
+    s = gpsplat.default_settings(width=320, height=180, samples_per_pixel=2)
+    batch = gpsplat.Batch(scene, s, 320, 180, 2, workers=1)
+    img = torch.empty((360, 640, 3), device="cuda")
+    dep = torch.empty((360, 640), device="cuda")
+    cam = gpsutil.cameras_for(s, synth.random_poses(1))[0]
+    with pytest.raises(gpsplat.GpsError) as e:
+        batch.render(gpsplat.Batch.views([(cam, 640, 360, 2, img.data_ptr(), dep.data_ptr())]))
+    assert e.value.status == 6
+    batch.close()
+    scene.close()
+
+
+def test_reset_makes_next_frame_a_fresh_render():
+    import torch
+
+    ply = gpsutil.cached_ply("town60k", lambda: synth.town(60000, seed=5))
+    scene = gpsplat.Scene.from_ply(ply)
+    s = gpsplat.default_settings(width=320, height=180, samples_per_pixel=2, max_number_of_points=4_000_000)
+    poses = synth.random_poses(2, seed=3)
+    cams = gpsutil.cameras_for(s, poses, first_frame=7)
+    _, want_img, want_dep = _plain(scene, dict(max_number_of_points=4_000_000), (poses[1], 320, 180, 2, 8))
+    r = gpsplat.Renderer(scene, s)
+    img = torch.empty((180, 320, 3), device="cuda")
+    dep = torch.empty((180, 320), device="cuda")
+    r.render(cams[0], img.data_ptr(), dep.data_ptr(), 0)
+    r.reset(0)
+    r.render(cams[1], img.data_ptr(), dep.data_ptr(), 0)
+    torch.cuda.synchronize()
+    assert np.array_equal(img.cpu().numpy().view(np.uint32), want_img.view(np.uint32))
+    assert np.array_equal(dep.cpu().numpy().view(np.uint32), want_dep.view(np.uint32))
+    r.close()
+    scene.close()
