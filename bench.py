@@ -144,7 +144,8 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def dist_init():
+def dist_init(backend: str = "nccl"):
+    """Replica plumbing: one process per GPU (RANK / LOCAL_RANK / WORLD_SIZE from torchrun)."""
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -153,17 +154,24 @@ def dist_init():
 
         import torch.distributed as dist
 
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=300))
     return world, rank, local
 
 
+def orbit_phase(rank: int, world: int, frames: int) -> int:
+    """First orbit keyframe of a replica: the ranks start evenly spread around the orbit."""
+    return (rank * frames) // max(1, world)
+
+
 def max_over_ranks(x: float, world: int) -> float:
+    """Device time of the job = the slowest replica's (all ranks take part, in the same order)."""
     if world == 1:
         return x
     import torch
     import torch.distributed as dist
 
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 
@@ -384,7 +392,7 @@ def main():
     r = gpsplat.Renderer(scene, s)
     loop = gpsplat.FrameLoop(r)
     poses = poses_for(spec)
-    phase = (rank * len(poses)) // max(1, world)
+    phase = orbit_phase(rank, world, len(poses))
     total = args.warmup + args.steps
     cams = make_cameras(gpsplat, s, poses, total, phase)
     stream = torch.cuda.Stream()
