@@ -46,6 +46,9 @@ def workload_spec(name: str):
     if name == "town4m":  # profiling-size variant of the headline workload
         return dict(n=4_000_000, kind="town", width=1920, height=1080, ss=2, spp=4, reduce=1, hier=1, occl=1,
                     taa=1, frames=120)
+    if name == "town256m":  # the town tiled 4 x 4 in the half-precision format
+        return dict(n=16_000_000, tiles=4, kind="town", fmt="half", width=1920, height=1080, ss=2, spp=4, reduce=1,
+                    hier=1, occl=1, taa=1, frames=120)
     if name == "cube1m":
         return dict(n=1_000_000, kind="cube", width=640, height=360, ss=1, spp=1, reduce=1, hier=0, occl=0, taa=0,
                     frames=1)
@@ -362,7 +365,7 @@ def main():
     ap.add_argument("--steps", type=int, default=30)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="mine", choices=["mine", "reference"])
-    ap.add_argument("--workload", default="town16m", choices=["town16m", "town4m", "cube1m", "batch64"])
+    ap.add_argument("--workload", default="town16m", choices=["town16m", "town4m", "town256m", "cube1m", "batch64"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
@@ -386,7 +389,14 @@ def main():
     gpsplat.load_library()
     g_host = load_scene_host(spec)
     t = time.time()
-    scene = gpsplat.Scene.from_host(np.ascontiguousarray(g_host), presorted=True)
+    if spec.get("fmt") == "half":
+        base_scene = gpsplat.Scene.from_host(np.ascontiguousarray(g_host), gpsplat.GPS_SCENE_HALF, presorted=True)
+        k = spec["tiles"]
+        ext = synth.TOWN_EXTENT
+        scene = base_scene.tile([[(i - (k - 1) / 2) * ext, (j - (k - 1) / 2) * ext] for j in range(k) for i in range(k)])
+        base_scene.close()
+    else:
+        scene = gpsplat.Scene.from_host(np.ascontiguousarray(g_host), presorted=True)
     log(f"rank {rank}: scene uploaded in {time.time() - t:.1f}s")
     s = settings_for(gpsplat, spec)
     r = gpsplat.Renderer(scene, s)
@@ -506,6 +516,9 @@ def main():
         "points_per_frame": [st.num_points_one, st.num_points_two],
         "survivors_per_frame": [st.survivors_one, st.survivors_two],
     }
+    if spec.get("fmt") == "half":
+        line["dtype"] = "f16/fp8 storage, f32 arithmetic"
+        line["config"]["format"] = "half (GPS_SCENE_HALF), town tiled %dx%d" % (spec["tiles"], spec["tiles"])
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(gpsplat, g_host, spec, s, poses)
     if rank == 0:

@@ -194,6 +194,15 @@ __device__ __forceinline__ bool preprocess_one(const PreprocessArgs& a, const Sc
         const float dil = 0.3f * (float)fc.ss * (float)fc.ss;
         cov2d = cov2d + make_v3(dil, 0.0f, dil);
         float det = cov2d.x * cov2d.z - cov2d.y * cov2d.y;
+        double det64 = 0.0;
+        bool precise = false;
+        if constexpr (Scene::kFp64Conic) {
+            if (det < 1.0e-3f * cov2d.x * cov2d.z) {  // a*c - b^2 cancels: recompute in FP64
+                det64 = (double)cov2d.x * (double)cov2d.z - (double)cov2d.y * (double)cov2d.y;
+                det = (float)det64;
+                precise = true;
+            }
+        }
         if (det <= 0.0f) break;
         vec2 pixel_mean = make_v2((proj_mean.x * 0.5f + 0.5f) * (float)fc.up_width,
                                   (proj_mean.y * 0.5f + 0.5f) * (float)fc.up_height);
@@ -235,7 +244,9 @@ __device__ __forceinline__ bool preprocess_one(const PreprocessArgs& a, const Sc
 
         // per-Gaussian prologue of splatGaussianPoint (gaussian_point_splatting.cu:88-96)
         const uint64_t view_depth_bits = depth_key(view_z, fc.near_plane, fc.far_plane) << kDepthShift;
-        vec3 conic = conic_of(cov2d, 1.0f / det);
+        vec3 conic;
+        if (precise) conic = make_v3((float)(cov2d.z / det64), (float)(-cov2d.y / det64), (float)(cov2d.x / det64));
+        else conic = conic_of(cov2d, 1.0f / det);
         const float c0 = __fsqrt_rn(cov2d.x);
         const float c1 = cov2d.y / c0;
         const float c2 = __fsqrt_rn(cov2d.z - c1 * c1);
@@ -975,6 +986,94 @@ __global__ void __launch_bounds__(kHizThreads * kHizThreads) hiz_build_kernel(Hi
 }
 
 // ---------------------------------------------------------------------------------
+// Half-precision scene: encode from the FP32 arrays, tile copies (load time)
+// ---------------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t pack_h2(float lo, float hi) {
+    return (uint32_t)__half_as_ushort(__float2half_rn(lo)) | ((uint32_t)__half_as_ushort(__float2half_rn(hi)) << 16);
+}
+
+// origin of every kHalfOriginBlock Gaussians: the centre of their means' bounding box
+__global__ void half_origins_kernel(const float4* __restrict__ pos_op, uint32_t n, float4* __restrict__ origin) {
+    const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t begin = b * kHalfOriginBlock;
+    if (begin >= n) return;
+    const uint32_t end = min(begin + kHalfOriginBlock, n);
+    float3 lo = make_float3(INFINITY, INFINITY, INFINITY), hi = make_float3(-INFINITY, -INFINITY, -INFINITY);
+    for (uint32_t g = begin; g < end; ++g) {
+        const float4 p = pos_op[g];
+        lo = make_float3(fminf(lo.x, p.x), fminf(lo.y, p.y), fminf(lo.z, p.z));
+        hi = make_float3(fmaxf(hi.x, p.x), fmaxf(hi.y, p.y), fmaxf(hi.z, p.z));
+    }
+    origin[b] = make_float4(0.5f * (lo.x + hi.x), 0.5f * (lo.y + hi.y), 0.5f * (lo.z + hi.z), 0.0f);
+}
+
+__global__ void encode_half_kernel(const float4* __restrict__ pos_op, const float4* __restrict__ rot,
+                                   const float4* __restrict__ scale, const float4* __restrict__ sh,
+                                   const float4* __restrict__ origin, uint32_t n, uint4* __restrict__ rec,
+                                   uint4* __restrict__ scl, uint4* __restrict__ acq) {
+    const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= n) return;
+    const float4 p = pos_op[g], q = rot[g], c = scale[g], o = origin[g / kHalfOriginBlock];
+    rec[g] = make_uint4(pack_h2(p.x - o.x, p.y - o.y), pack_h2(p.z - o.z, p.w), pack_h2(q.x, q.y), pack_h2(q.z, q.w));
+    float v[48];
+#pragma unroll
+    for (int i = 0; i < 12; ++i) {
+        const float4 t = sh[(size_t)g * 12 + i];
+        v[4 * i] = t.x;
+        v[4 * i + 1] = t.y;
+        v[4 * i + 2] = t.z;
+        v[4 * i + 3] = t.w;
+    }
+    float m = 0.0f;
+#pragma unroll
+    for (int j = 3; j < 48; ++j) m = fmaxf(m, fabsf(v[j]));
+    const float k = m > 0.0f ? m / 448.0f : 1.0f;   // 448 = largest finite e4m3 value
+    scl[g] = make_uint4(pack_h2(c.x, c.y), pack_h2(c.z, v[0]), pack_h2(v[1], v[2]), __float_as_uint(k));
+    uint32_t w[12];
+#pragma unroll
+    for (int i = 0; i < 12; ++i) w[i] = 0u;
+#pragma unroll
+    for (int j = 0; j < 45; ++j) {
+        const uint32_t b = (uint32_t)__nv_cvt_float_to_fp8(v[3 + j] / k, __NV_SATFINITE, __NV_E4M3);
+        w[j >> 2] |= b << (8 * (j & 3));
+    }
+#pragma unroll
+    for (int i = 0; i < 3; ++i) acq[(size_t)g * 3 + i] = make_uint4(w[4 * i], w[4 * i + 1], w[4 * i + 2], w[4 * i + 3]);
+}
+
+// copies of a half scene: origins of copy k = source origins + (dx[k], 0, dz[k])
+__global__ void translate_origins_kernel(const float4* __restrict__ src, uint32_t count, float dx, float dz,
+                                         float4* __restrict__ dst) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= count) return;
+    const float4 o = src[i];
+    dst[i] = make_float4(o.x + dx, o.y, o.z + dz, o.w);
+}
+
+// cull blocks of the tiled scene: node j covers Gaussians [j*pb, j*pb+pb) inside one copy and is
+// the union of the source nodes it spans, translated with its copy
+__global__ void tile_nodes_kernel(const float4* __restrict__ src, uint32_t src_pb, uint32_t src_n, uint32_t pb,
+                                  uint32_t copies, const float2* __restrict__ offsets, uint64_t total,
+                                  float4* __restrict__ dst, uint32_t nodes) {
+    const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= nodes) return;
+    const uint64_t begin = (uint64_t)j * pb;
+    const uint64_t end = min(begin + pb, total);
+    const uint32_t k = (uint32_t)(begin / src_n);
+    const uint32_t s0 = (uint32_t)((begin - (uint64_t)k * src_n) / src_pb);
+    const uint32_t s1 = (uint32_t)((end - 1 - (uint64_t)k * src_n) / src_pb);
+    float3 lo = make_float3(INFINITY, INFINITY, INFINITY), hi = make_float3(-INFINITY, -INFINITY, -INFINITY);
+    for (uint32_t s = s0; s <= s1; ++s) {
+        const float4 a = src[2 * s], b = src[2 * s + 1];
+        lo = make_float3(fminf(lo.x, a.x), fminf(lo.y, a.y), fminf(lo.z, a.z));
+        hi = make_float3(fmaxf(hi.x, b.x), fmaxf(hi.y, b.y), fmaxf(hi.z, b.z));
+    }
+    const float2 t = offsets[k];
+    dst[2 * j] = make_float4(lo.x + t.x, lo.y, lo.z + t.y, __uint_as_float((uint32_t)begin));
+    dst[2 * j + 1] = make_float4(hi.x + t.x, hi.y, hi.z + t.y, __uint_as_float((uint32_t)(end - begin)));
+}
+
+// ---------------------------------------------------------------------------------
 // Block AABBs at load time (gaussian_bvh.cu:111-144).  The reference computes these on the
 // host in IEEE single precision without fused multiply-adds; the _rn intrinsics below keep
 // nvcc from contracting, so the boxes are bit-identical to the host computation.
@@ -1170,6 +1269,11 @@ void launch_preprocess_fp32(const PreprocessArgs& a, const SceneFP32& s, cudaStr
     preprocess_kernel<SceneFP32><<<preprocess_grid_size<SceneFP32>(a.n), 256, 0, stream>>>(a, s);
 }
 
+void launch_preprocess_half(const PreprocessArgs& a, const SceneHalf& s, cudaStream_t stream) {
+    if (a.n == 0) return;
+    preprocess_kernel<SceneHalf><<<preprocess_grid_size<SceneHalf>(a.n), 256, 0, stream>>>(a, s);
+}
+
 void launch_preprocess_compressed(const PreprocessArgs& a, const SceneCompressed& s, cudaStream_t stream) {
     if (a.n == 0) return;
     preprocess_kernel<SceneCompressed><<<preprocess_grid_size<SceneCompressed>(a.n), 256, 0, stream>>>(a, s);
@@ -1268,6 +1372,23 @@ void launch_hiz_build(const HizView& h, const float* depth, int min_levels, cuda
     const int L = h.levels - 1;
     dim3 grid((h.level_w[L] + kHizTile - 1) / kHizTile, (h.level_h[L] + kHizTile - 1) / kHizTile);
     hiz_build_kernel<<<grid, kHizThreads * kHizThreads, 0, stream>>>(h, depth, min_levels);
+}
+
+void launch_encode_half(const float4* pos_op, const float4* rot, const float4* scale, const float4* sh, uint32_t n,
+                        float4* origin, uint4* rec, uint4* scl, uint4* acq, cudaStream_t stream) {
+    if (n == 0) return;
+    const uint32_t blocks = (n + kHalfOriginBlock - 1) / kHalfOriginBlock;
+    half_origins_kernel<<<(blocks + 255) / 256, 256, 0, stream>>>(pos_op, n, origin);
+    encode_half_kernel<<<(n + 255) / 256, 256, 0, stream>>>(pos_op, rot, scale, sh, origin, n, rec, scl, acq);
+}
+
+void launch_translate_origins(const float4* src, uint32_t count, float dx, float dz, float4* dst, cudaStream_t stream) {
+    if (count) translate_origins_kernel<<<(count + 255) / 256, 256, 0, stream>>>(src, count, dx, dz, dst);
+}
+
+void launch_tile_nodes(const float4* src, uint32_t src_pb, uint32_t src_n, uint32_t pb, uint32_t copies,
+                       const float2* offsets, uint64_t total, float4* dst, uint32_t nodes, cudaStream_t stream) {
+    if (nodes) tile_nodes_kernel<<<(nodes + 255) / 256, 256, 0, stream>>>(src, src_pb, src_n, pb, copies, offsets, total, dst, nodes);
 }
 
 void launch_block_bounds(const float4* pos_op, const float4* rot, const float4* scale, uint32_t n,

@@ -125,6 +125,13 @@ void launch_block_cull(const BlockView& b, const FrameConst& fc, const HizView& 
 void launch_visible_chunks(const BlockView& b, uint32_t n, uint32_t* list, uint32_t* mask_cur, cudaStream_t stream);
 void launch_preprocess_fp32(const PreprocessArgs& a, const SceneFP32& s, cudaStream_t stream);
 void launch_preprocess_compressed(const PreprocessArgs& a, const SceneCompressed& s, cudaStream_t stream);
+void launch_preprocess_half(const PreprocessArgs& a, const SceneHalf& s, cudaStream_t stream);
+// half-precision scenes (load time)
+void launch_encode_half(const float4* pos_op, const float4* rot, const float4* scale, const float4* sh, uint32_t n,
+                        float4* origin, uint4* rec, uint4* scl, uint4* acq, cudaStream_t stream);
+void launch_translate_origins(const float4* src, uint32_t count, float dx, float dz, float4* dst, cudaStream_t stream);
+void launch_tile_nodes(const float4* src, uint32_t src_pb, uint32_t src_n, uint32_t pb, uint32_t copies,
+                       const float2* offsets, uint64_t total, float4* dst, uint32_t nodes, cudaStream_t stream);
 void launch_scan(const ScanArgs& a, uint32_t scan_tiles, cudaStream_t stream);
 uint32_t scan_tile_count(uint32_t n);
 void launch_splat(const SplatArgs& a, int grid, int block, cudaStream_t stream);

@@ -13,6 +13,8 @@
 // evaluation follows sh.cuh:191-223 (FP32) and sh.cuh:41-47,55-96,257-273 (compact).
 #pragma once
 #include <cstdint>
+#include <cuda_fp16.h>
+#include <cuda_fp8.h>
 #include <cuda_runtime.h>
 #include "gps_math.cuh"
 
@@ -133,6 +135,7 @@ struct SceneFP32 {
     const float4* __restrict__ scale;
     const float4* __restrict__ sh;
     uint32_t n;
+    static constexpr bool kFp64Conic = false;
 
 #if defined(__CUDACC__)
     GPS_D float opacity(uint32_t g) const {
@@ -172,6 +175,7 @@ struct SceneCompressed {
     const uint4* __restrict__ sh_ac;
     SceneBounds bounds;
     uint32_t n;
+    static constexpr bool kFp64Conic = false;
 
 #if defined(__CUDACC__)
     GPS_D float opacity(uint32_t g) const {
@@ -248,6 +252,65 @@ struct SceneCompressed {
         }
         result = result + make_v3(0.5f, 0.5f, 0.5f);
         return vmax0(result);
+    }
+#endif
+};
+
+// Half-precision storage (this library's own format, no counterpart in the reference), 80 bytes
+// per Gaussian, decoded to FP32 for all arithmetic:
+//   rec   uint4 : FP16 position relative to its block origin (x, y, z), FP16 opacity,
+//                 FP16 rotation (w, x, y, z)
+//   scl   uint4 : FP16 scale (x, y, z), FP16 SH DC term (r, g, b), FP32 AC scale k
+//   ac    3 x uint4 : the 45 AC SH coefficients (FP32 layout order 3..47) as FP8 e4m3 of
+//                 value / k, k = max |AC| / 448; 3 pad bytes
+//   origin float4 per kHalfOriginBlock Gaussians: the block's position origin
+// The DC term carries most of a Gaussian's colour, so it keeps 11 significant bits.
+constexpr uint32_t kHalfOriginBlock = 16;
+
+struct SceneHalf {
+    const uint4* __restrict__ rec;
+    const uint4* __restrict__ scl;
+    const uint4* __restrict__ ac;
+    const float4* __restrict__ origin;
+    uint32_t n;
+    // near-degenerate 2D covariances (det small against a*c) are inverted in FP64
+    static constexpr bool kFp64Conic = true;
+
+#if defined(__CUDACC__)
+    static GPS_D float h(uint32_t word, int hi) {
+        return __half2float(__ushort_as_half((unsigned short)(hi ? (word >> 16) : (word & 0xFFFFu))));
+    }
+    GPS_D float opacity(uint32_t g) const { return gmin(h(__ldg(&rec[g]).y, 1), kMaxOpacity); }
+    GPS_D void geometry(uint32_t g, vec3& mean, vec4& quat, vec3& s) const {
+        const uint4 r = __ldg(&rec[g]);
+        const uint4 c = __ldg(&scl[g]);
+        const float4 o = __ldg(&origin[g / kHalfOriginBlock]);
+        mean = make_v3(o.x + h(r.x, 0), o.y + h(r.x, 1), o.z + h(r.y, 0));
+        quat = make_v4(h(r.z, 0), h(r.z, 1), h(r.w, 0), h(r.w, 1));
+        s = make_v3(h(c.x, 0), h(c.x, 1), h(c.y, 0));
+    }
+    GPS_D vec3 color(uint32_t g, vec3 mean, vec3 campos) const {
+        float shs_[48];
+        const uint4 c = __ldg(&scl[g]);
+        shs_[0] = h(c.y, 1);
+        shs_[1] = h(c.z, 0);
+        shs_[2] = h(c.z, 1);
+        const float k = __uint_as_float(c.w);
+        const uint4* src = ac + (size_t)g * 3;
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+            const uint4 v = __ldg(&src[i]);
+            const uint32_t w[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+            for (int j = 0; j < 16; ++j) {
+                const int e = 16 * i + j;
+                if (e >= 45) break;
+                __nv_fp8_e4m3 q;
+                q.__x = (__nv_fp8_storage_t)((w[j >> 2] >> (8 * (j & 3))) & 0xFFu);
+                shs_[3 + e] = (float)q * k;
+            }
+        }
+        return color_from_sh_fp32(mean, campos, shs_);
     }
 #endif
 };

@@ -90,6 +90,9 @@ struct gps_scene {
     dptr<uint4> geom, sh_ac;
     dptr<uint8_t> opac;
     dptr<float4> sh_dc;
+    // half-precision arrays
+    dptr<uint4> h_rec, h_scl, h_ac;
+    dptr<float4> h_origin;
     SceneBounds bounds{};
     // fixed-size blocks for the hierarchical cull (computed from the FP32 values, like
     // build_fixed_blocks on the host CPUGaussian array)
@@ -116,7 +119,7 @@ void scene_upload(gps_scene* s, const CpuGaussian* g, uint64_t n) {
     float4* d_scale = dev_alloc<float4>(n);
     s->scale.reset(d_scale);
     float4* d_sh = nullptr;
-    if (s->format == GPS_SCENE_FP32) {
+    if (s->format == GPS_SCENE_FP32 || s->format == GPS_SCENE_HALF) {
         d_sh = dev_alloc<float4>(n * 12);
         s->sh.reset(d_sh);
     }
@@ -142,6 +145,20 @@ void scene_upload(gps_scene* s, const CpuGaussian* g, uint64_t n) {
     s->block_nodes.reset(nodes);
     launch_block_bounds(d_pos, d_rot, d_scale, (uint32_t)n, s->per_block, nodes, 0);
     GPS_CUDA(cudaGetLastError());
+    if (s->format == GPS_SCENE_HALF) {
+        s->h_rec.reset(dev_alloc<uint4>(n));
+        s->h_scl.reset(dev_alloc<uint4>(n));
+        s->h_ac.reset(dev_alloc<uint4>(n * 3));
+        s->h_origin.reset(dev_alloc<float4>((n + kHalfOriginBlock - 1) / kHalfOriginBlock));
+        launch_encode_half(d_pos, d_rot, d_scale, d_sh, (uint32_t)n, s->h_origin.get(), s->h_rec.get(), s->h_scl.get(),
+                           s->h_ac.get(), 0);
+        GPS_CUDA(cudaGetLastError());
+        GPS_CUDA(cudaDeviceSynchronize());
+        s->pos_op.reset();
+        s->rot.reset();
+        s->scale.reset();
+        s->sh.reset();
+    }
     if (s->format == GPS_SCENE_COMPRESSED) {
         s->bounds = compute_scene_bounds(g, n);
         std::vector<uint4> geom(n), ac(n * 3);
@@ -342,6 +359,9 @@ void render_pass(gps_renderer* r, const FrameConst& fc, int frame, bool first, c
     if (r->scene->format == GPS_SCENE_FP32) {
         SceneFP32 s{r->scene->pos_op.get(), r->scene->rot.get(), r->scene->scale.get(), r->scene->sh.get(), r->n};
         launch_preprocess_fp32(pa, s, st);
+    } else if (r->scene->format == GPS_SCENE_HALF) {
+        SceneHalf s{r->scene->h_rec.get(), r->scene->h_scl.get(), r->scene->h_ac.get(), r->scene->h_origin.get(), r->n};
+        launch_preprocess_half(pa, s, st);
     } else {
         SceneCompressed s{};
         s.geom = r->scene->geom.get();
@@ -476,7 +496,8 @@ gps_status gps_settings_parse_args(int32_t argc, const char* const* argv, gps_se
 }
 
 static gps_status scene_create(std::vector<CpuGaussian>& g, int32_t format, bool presorted, gps_scene** out) {
-    if (format != GPS_SCENE_FP32 && format != GPS_SCENE_COMPRESSED) return fail(GPS_ERR_INVALID_ARGUMENT, "unknown scene format");
+    if (format != GPS_SCENE_FP32 && format != GPS_SCENE_COMPRESSED && format != GPS_SCENE_HALF)
+        return fail(GPS_ERR_INVALID_ARGUMENT, "unknown scene format");
     if (g.size() >= (1ull << 30)) return fail(GPS_ERR_SIZE, "scenes are limited to 2^30 Gaussians");
     auto s = std::make_unique<gps_scene>();
     s->format = format;
@@ -518,6 +539,48 @@ gps_status gps_scene_from_host(const float* gaussians, uint64_t count, int32_t f
 
 uint64_t gps_scene_count(const gps_scene* scene) { return scene ? scene->n : 0; }
 int32_t gps_scene_format_of(const gps_scene* scene) { return scene ? scene->format : -1; }
+
+gps_status gps_scene_tile(const gps_scene* src, int32_t copies, const float* offsets_xz, gps_scene** out) {
+    if (!src || !offsets_xz || !out || copies < 1) return fail(GPS_ERR_INVALID_ARGUMENT, "bad argument");
+    *out = nullptr;
+    if (src->format != GPS_SCENE_HALF) return fail(GPS_ERR_INVALID_ARGUMENT, "only GPS_SCENE_HALF scenes can be tiled");
+    const uint64_t n = src->n, total = n * (uint64_t)copies;
+    if (total >= (1ull << 30)) return fail(GPS_ERR_SIZE, "scenes are limited to 2^30 Gaussians");
+    if (n % kHalfOriginBlock) return fail(GPS_ERR_INVALID_ARGUMENT, "the source count must be a multiple of 16");
+    auto s = std::make_unique<gps_scene>();
+    s->format = GPS_SCENE_HALF;
+    s->n = total;
+    s->presorted = src->presorted;
+    uint32_t pb = gaussians_per_block(total);
+    if (n % pb || pb % src->per_block) pb = src->per_block;   // blocks must not straddle copies
+    s->per_block = pb;
+    s->block_count = (uint32_t)((total + pb - 1) / pb);
+    try {
+        const uint64_t ob = n / kHalfOriginBlock;
+        s->h_rec.reset(dev_alloc<uint4>(total));
+        s->h_scl.reset(dev_alloc<uint4>(total));
+        s->h_ac.reset(dev_alloc<uint4>(total * 3));
+        s->h_origin.reset(dev_alloc<float4>(ob * copies));
+        s->block_nodes.reset(dev_alloc<float4>((size_t)s->block_count * 2));
+        dptr<float2> offs(dev_alloc<float2>(copies));
+        GPS_CUDA(cudaMemcpy(offs.get(), offsets_xz, sizeof(float2) * copies, cudaMemcpyHostToDevice));
+        for (int32_t k = 0; k < copies; ++k) {
+            GPS_CUDA(cudaMemcpy(s->h_rec.get() + k * n, src->h_rec.get(), n * sizeof(uint4), cudaMemcpyDeviceToDevice));
+            GPS_CUDA(cudaMemcpy(s->h_scl.get() + k * n, src->h_scl.get(), n * sizeof(uint4), cudaMemcpyDeviceToDevice));
+            GPS_CUDA(cudaMemcpy(s->h_ac.get() + k * n * 3, src->h_ac.get(), n * 3 * sizeof(uint4), cudaMemcpyDeviceToDevice));
+            launch_translate_origins(src->h_origin.get(), (uint32_t)ob, offsets_xz[2 * k], offsets_xz[2 * k + 1],
+                                     s->h_origin.get() + k * ob, 0);
+        }
+        launch_tile_nodes(src->block_nodes.get(), src->per_block, (uint32_t)n, pb, (uint32_t)copies, offs.get(), total,
+                          s->block_nodes.get(), s->block_count, 0);
+        GPS_CUDA(cudaGetLastError());
+        GPS_CUDA(cudaDeviceSynchronize());
+    } catch (const CudaError& e) {
+        return fail(std::string(e.what()).find("cudaMalloc") != std::string::npos ? GPS_ERR_OUT_OF_MEMORY : GPS_ERR_CUDA, e.what());
+    }
+    *out = s.release();
+    return GPS_OK;
+}
 void gps_scene_free(gps_scene* scene) { delete scene; }
 
 gps_status gps_ply_write(const char* path, const float* gaussians, uint64_t count, const char* comments) {

@@ -21,6 +21,7 @@ LIB_PATH = os.environ.get("GPS_B200_LIBRARY") or os.path.join(_HERE, "libgps_b20
 
 GPS_SCENE_FP32 = 0
 GPS_SCENE_COMPRESSED = 1
+GPS_SCENE_HALF = 2
 GPS_ACCUM_PROGRESSIVE = 0
 GPS_ACCUM_TAA = 1
 GPS_ACCUM_NONE = 2
@@ -144,6 +145,7 @@ _SIGNATURES = [
     ("gps_settings_parse_args", c_int32, [c_int32, POINTER(c_char_p), POINTER(Settings), c_char_p, ctypes.c_size_t, c_char_p, ctypes.c_size_t]),
     ("gps_scene_load_ply", c_int32, [c_char_p, c_int32, c_int32, POINTER(c_void_p), POINTER(c_int32)]),
     ("gps_scene_from_host", c_int32, [c_void_p, c_uint64, c_int32, c_int32, POINTER(c_void_p)]),
+    ("gps_scene_tile", c_int32, [c_void_p, c_int32, POINTER(c_float), POINTER(c_void_p)]),
     ("gps_scene_count", c_uint64, [c_void_p]),
     ("gps_scene_format_of", c_int32, [c_void_p]),
     ("gps_scene_free", None, [c_void_p]),
@@ -315,6 +317,13 @@ class Scene:
         h = c_void_p()
         _check(load_library().gps_scene_from_host(g.ctypes.data, g.shape[0], fmt, int(presorted), byref(h)))
         return cls(h, presorted)
+
+    def tile(self, offsets_xz) -> "Scene":
+        """A half-precision scene of translated copies of this one (gps_scene_tile)."""
+        off = np.ascontiguousarray(np.asarray(offsets_xz, np.float32).reshape(-1, 2))
+        h = c_void_p()
+        _check(load_library().gps_scene_tile(self._h, off.shape[0], off.ctypes.data_as(POINTER(c_float)), byref(h)))
+        return Scene(h, self.presorted)
 
     @property
     def count(self) -> int:

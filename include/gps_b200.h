@@ -36,8 +36,15 @@ typedef enum gps_status {
 /* Scene storage formats on the device. */
 typedef enum gps_scene_format {
     GPS_SCENE_FP32 = 0,        /* GPUGaussianSceneUncompressed (gaussian_types.cuh:548-646) */
-    GPS_SCENE_COMPRESSED = 1   /* GPUGaussianSceneCompressed, the reference's default build
+    GPS_SCENE_COMPRESSED = 1,  /* GPUGaussianSceneCompressed, the reference's default build
                                   (config.h:15, gaussian_types.cuh:421-541) */
+    GPS_SCENE_HALF = 2         /* this library's own storage, no counterpart in the reference:
+                                  FP16 position (relative to a 16-Gaussian block origin), opacity,
+                                  rotation, scale and SH DC term, FP8 e4m3 SH AC terms with a
+                                  per-Gaussian FP32 scale; 80 bytes per Gaussian (FP32: 240),
+                                  decoded to FP32, near-degenerate 2D
+                                  covariances inverted in FP64.  Not bit-exact with the
+                                  reference by design. */
 } gps_scene_format;
 
 typedef enum gps_accumulation {
@@ -128,6 +135,11 @@ gps_status gps_scene_load_ply(const char* path, int32_t format, int32_t sort_mor
  * scale[3] (activated), rotation[4] (normalised, rot_0..rot_3). */
 gps_status gps_scene_from_host(const float* gaussians, uint64_t count, int32_t format,
                                int32_t presorted, gps_scene** out);
+/* A new GPS_SCENE_HALF scene holding `copies` translated copies of a GPS_SCENE_HALF scene (copy
+ * k moved by (offsets_xz[2k], 0, offsets_xz[2k+1])), built on the device; the culling blocks
+ * follow the reference's size rule for the new count (like GaussianEditor::Repeat,
+ * src/core/gaussians/editor/gaussian_editor.cu:37-65, followed by build_fixed_blocks). */
+gps_status gps_scene_tile(const gps_scene* src, int32_t copies, const float* offsets_xz, gps_scene** out);
 uint64_t gps_scene_count(const gps_scene* scene);
 int32_t gps_scene_format_of(const gps_scene* scene);
 void gps_scene_free(gps_scene* scene);
