@@ -2,7 +2,7 @@
 //
 //   block cull    gaussian_bvh.cu:215-329          one thread per block node, warp ballot
 //   preprocess    gaussian_point_splatting.cu:17-65,147-307
-//   scan          workload_distributor.cu:52-145   single-pass decoupled look-back scan that
+//   scan          workload_distributor.cu:52-145   tile reduce -> tile scan -> downsweep that
 //                                                  compacts survivors and keeps P on the device
 //   splat         gaussian_point_splatting.cu:67-141,383-432  persistent, tile-of-points blocks
 //   clear/resolve gaussian_point_splatting.cu:484-548,580-585
@@ -27,7 +27,6 @@ namespace {
 constexpr int kScanThreads = 256;
 constexpr int kScanItems = 16;
 constexpr uint32_t kScanTile = kScanThreads * kScanItems;  // 4096 Gaussians per scan tile
-constexpr int kSpinLimit = 1 << 22;                         // bounded look-back wait
 
 // ---------------------------------------------------------------------------------
 // Hi-Z query (depth_mip_chain.cuh:172-215, the non-tree variant the reference compiles)
@@ -295,31 +294,16 @@ __global__ void __launch_bounds__(256) preprocess_kernel(PreprocessArgs a, Scene
 }
 
 // ---------------------------------------------------------------------------------
-// Scan: single-pass decoupled look-back over (survivor count, point count) pairs
-// (replaces workload_distributor.cu:62-145: 3 blocking D2H copies, an exclusive scan,
-// a scatter and a P-long max-scan).  Status word: [63:62] flag, [61:32] survivors,
-// [31:0] points (mod 2^32 like the reference's u32 offsets).
+// Scan over (survivor count, point count) pairs in three fully parallel launches: per-tile
+// totals, one block scanning the tile totals, a downsweep writing the compacted survivors
+// (replaces workload_distributor.cu:62-145: 3 blocking D2H copies, an exclusive scan, a
+// scatter and a P-long max-scan).  Tile word: [63:32] survivors, [31:0] points (mod 2^32 like
+// the reference's u32 offsets).  No block waits on another, so there is no spin at all.
 // ---------------------------------------------------------------------------------
-constexpr unsigned long long kFlagAgg = 1ull << 62;
-constexpr unsigned long long kFlagInc = 2ull << 62;
 
-__device__ __forceinline__ unsigned long long pack_status(unsigned long long flag, uint32_t surv, uint32_t pts) {
-    return flag | ((unsigned long long)(surv & 0x3FFFFFFFu) << 32) | pts;
-}
-
-__global__ void __launch_bounds__(kScanThreads) scan_kernel(ScanArgs a) {
-    __shared__ uint32_t s_tile;
-    __shared__ uint32_t s_warp_surv[kScanThreads / 32];
-    __shared__ uint32_t s_warp_pts[kScanThreads / 32];
-    __shared__ uint32_t s_prefix_surv, s_prefix_pts;
-    if (threadIdx.x == 0) s_tile = atomicAdd(a.tile_ticket, 1u);
-    __syncthreads();
-    const uint32_t tile = s_tile;
-    const uint32_t num_tiles = (a.n + kScanTile - 1) / kScanTile;
-    const uint32_t base = tile * kScanTile + threadIdx.x * kScanItems;
-
+// One scan tile (4096 Gaussians, 16 per thread): the thread's mask bits and point counts.
+__device__ __forceinline__ uint32_t scan_load(const ScanArgs& a, uint32_t base, uint32_t cnt[kScanItems]) {
     uint32_t bits = 0;
-    uint32_t cnt[kScanItems];
     if (base < a.n) {
         bits = (__ldg(&a.mask[base >> 5]) >> (base & 31)) & 0xFFFFu;
         if (a.n - base < (uint32_t)kScanItems) bits &= (1u << (a.n - base)) - 1u;
@@ -333,104 +317,105 @@ __global__ void __launch_bounds__(kScanThreads) scan_kernel(ScanArgs a) {
         cnt[4 * q + 2] = ((bits >> (4 * q + 2)) & 1u) ? v.z : 0u;
         cnt[4 * q + 3] = ((bits >> (4 * q + 3)) & 1u) ? v.w : 0u;
     }
-    uint32_t t_surv = __popc(bits);
-    uint32_t t_pts = 0;
-#pragma unroll
-    for (int i = 0; i < kScanItems; ++i) t_pts += cnt[i];
+    return bits;
+}
 
-    // block-wide inclusive scan of the per-thread aggregates
+// Block-wide exclusive scan of (survivors, points) pairs; also returns the block totals.
+template <int kThreads>
+__device__ __forceinline__ void block_scan_pair(uint32_t s, uint32_t p, uint32_t& ex_s, uint32_t& ex_p,
+                                                uint32_t& tot_s, uint32_t& tot_p) {
+    __shared__ uint32_t w_s[kThreads / 32], w_p[kThreads / 32];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    uint32_t inc_surv = t_surv, inc_pts = t_pts;
+    uint32_t is = s, ip = p;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
-        uint32_t vs = __shfl_up_sync(0xffffffffu, inc_surv, o);
-        uint32_t vp = __shfl_up_sync(0xffffffffu, inc_pts, o);
+        const uint32_t vs = __shfl_up_sync(0xffffffffu, is, o);
+        const uint32_t vp = __shfl_up_sync(0xffffffffu, ip, o);
         if (lane >= o) {
-            inc_surv += vs;
-            inc_pts += vp;
+            is += vs;
+            ip += vp;
         }
     }
     if (lane == 31) {
-        s_warp_surv[warp] = inc_surv;
-        s_warp_pts[warp] = inc_pts;
+        w_s[warp] = is;
+        w_p[warp] = ip;
     }
     __syncthreads();
-    uint32_t warp_off_surv = 0, warp_off_pts = 0, blk_surv = 0, blk_pts = 0;
+    uint32_t off_s = 0, off_p = 0, all_s = 0, all_p = 0;
 #pragma unroll
-    for (int w = 0; w < kScanThreads / 32; ++w) {
+    for (int w = 0; w < kThreads / 32; ++w) {
         if (w < warp) {
-            warp_off_surv += s_warp_surv[w];
-            warp_off_pts += s_warp_pts[w];
+            off_s += w_s[w];
+            off_p += w_p[w];
         }
-        blk_surv += s_warp_surv[w];
-        blk_pts += s_warp_pts[w];
+        all_s += w_s[w];
+        all_p += w_p[w];
     }
-    uint32_t ex_surv = warp_off_surv + inc_surv - t_surv;
-    uint32_t ex_pts = warp_off_pts + inc_pts - t_pts;
+    ex_s = off_s + is - s;
+    ex_p = off_p + ip - p;
+    tot_s = all_s;
+    tot_p = all_p;
+}
 
-    // decoupled look-back (warp 0)
-    volatile unsigned long long* state = a.tile_state;
-    if (warp == 0) {
-        uint32_t pre_surv = 0, pre_pts = 0;
-        if (tile == 0) {
-            if (lane == 0) state[0] = pack_status(kFlagInc, blk_surv, blk_pts);
-        } else {
-            if (lane == 0) state[tile] = pack_status(kFlagAgg, blk_surv, blk_pts);
-            int window_end = (int)tile - 1;  // look at tiles window_end - lane
-            bool done = false;
-            bool timeout = false;
-            while (!done) {
-                int t = window_end - lane;
-                unsigned long long s = 0;
-                if (t >= 0) {
-                    int spins = 0;
-                    s = state[t];
-                    while ((s >> 62) == 0ull) {
-                        if (++spins > kSpinLimit) {
-                            timeout = true;
-                            break;
-                        }
-                        __nanosleep(64);
-                        s = state[t];
-                    }
-                } else {
-                    s = kFlagInc;  // virtual inclusive zero before tile 0
-                }
-                if (__any_sync(0xffffffffu, timeout)) {
-                    if (lane == 0) atomicExch(&a.counters->scan_timeouts, 1u);
-                    break;
-                }
-                unsigned inc_mask = __ballot_sync(0xffffffffu, (s >> 62) == 2ull);
-                int first_inc = inc_mask ? __ffs(inc_mask) - 1 : 32;  // closest tile with inclusive prefix
-                uint32_t vs = (lane <= first_inc) ? (uint32_t)((s >> 32) & 0x3FFFFFFFu) : 0u;
-                uint32_t vp = (lane <= first_inc) ? (uint32_t)(s & 0xFFFFFFFFu) : 0u;
+// Pass 1 of the scan: every tile's survivor and point totals, fully parallel.
+__global__ void __launch_bounds__(kScanThreads) scan_reduce_kernel(ScanArgs a) {
+    const uint32_t tile = blockIdx.x;
+    uint32_t cnt[kScanItems];
+    const uint32_t bits = scan_load(a, tile * kScanTile + threadIdx.x * kScanItems, cnt);
+    uint32_t pts = 0;
 #pragma unroll
-                for (int o = 16; o > 0; o >>= 1) {
-                    vs += __shfl_xor_sync(0xffffffffu, vs, o);
-                    vp += __shfl_xor_sync(0xffffffffu, vp, o);
-                }
-                pre_surv += vs;
-                pre_pts += vp;
-                if (inc_mask) done = true;
-                else window_end -= 32;
-            }
-            if (lane == 0) state[tile] = pack_status(kFlagInc, pre_surv + blk_surv, pre_pts + blk_pts);
-        }
-        if (lane == 0) {
-            s_prefix_surv = pre_surv;
-            s_prefix_pts = pre_pts;
-            if (tile == num_tiles - 1) {
-                uint32_t total = pre_pts + blk_pts;
-                a.counters->survivors = pre_surv + blk_surv;
-                a.counters->total_points = total;
-                a.counters->points = total < a.max_points ? total : a.max_points;
-                a.counters->truncated = total > a.max_points ? 1u : 0u;
-            }
-        }
+    for (int i = 0; i < kScanItems; ++i) pts += cnt[i];
+    uint32_t ex_s, ex_p, tot_s, tot_p;
+    block_scan_pair<kScanThreads>(__popc(bits), pts, ex_s, ex_p, tot_s, tot_p);
+    if (threadIdx.x == 0) a.tile_state[tile] = ((unsigned long long)tot_s << 32) | tot_p;
+}
+
+// Pass 2: one block turns the tile totals into exclusive tile prefixes (in place) and writes
+// the pass counters (points mod 2^32, like the reference's u32 offsets).
+constexpr int kTileScanThreads = 1024;
+__global__ void __launch_bounds__(kTileScanThreads) scan_tiles_kernel(ScanArgs a, uint32_t num_tiles) {
+    const uint32_t per = (num_tiles + kTileScanThreads - 1) / kTileScanThreads;
+    const uint32_t t0 = min(threadIdx.x * per, num_tiles), t1 = min(t0 + per, num_tiles);
+    uint32_t s = 0, p = 0;
+    for (uint32_t t = t0; t < t1; ++t) {
+        const unsigned long long v = a.tile_state[t];
+        s += (uint32_t)(v >> 32);
+        p += (uint32_t)v;
     }
-    __syncthreads();
-    uint32_t r = s_prefix_surv + ex_surv;
-    uint32_t pt = s_prefix_pts + ex_pts;
+    uint32_t ex_s, ex_p, tot_s, tot_p;
+    block_scan_pair<kTileScanThreads>(s, p, ex_s, ex_p, tot_s, tot_p);
+    for (uint32_t t = t0; t < t1; ++t) {
+        const unsigned long long v = a.tile_state[t];
+        a.tile_state[t] = ((unsigned long long)ex_s << 32) | ex_p;
+        ex_s += (uint32_t)(v >> 32);
+        ex_p += (uint32_t)v;
+    }
+    if (threadIdx.x == 0) {
+        a.counters->survivors = tot_s;
+        a.counters->total_points = tot_p;
+        a.counters->points = tot_p < a.max_points ? tot_p : a.max_points;
+        a.counters->truncated = tot_p > a.max_points ? 1u : 0u;
+        a.counters->scan_timeouts = 0u;
+        a.counters->pad[0] = a.counters->pad[1] = a.counters->pad[2] = 0u;
+    }
+}
+
+// Pass 3: each tile rescans its Gaussians from its prefix and writes the compacted survivor
+// ids and first points.
+__global__ void __launch_bounds__(kScanThreads) scan_write_kernel(ScanArgs a) {
+    const uint32_t tile = blockIdx.x;
+    const uint32_t base = tile * kScanTile + threadIdx.x * kScanItems;
+    uint32_t cnt[kScanItems];
+    const uint32_t bits = scan_load(a, base, cnt);
+    uint32_t pts = 0;
+#pragma unroll
+    for (int i = 0; i < kScanItems; ++i) pts += cnt[i];
+    uint32_t ex_s, ex_p, tot_s, tot_p;
+    block_scan_pair<kScanThreads>(__popc(bits), pts, ex_s, ex_p, tot_s, tot_p);
+    if (bits == 0u) return;
+    const unsigned long long pre = a.tile_state[tile];
+    uint32_t r = (uint32_t)(pre >> 32) + ex_s;
+    uint32_t pt = (uint32_t)pre + ex_p;
 #pragma unroll
     for (int i = 0; i < kScanItems; ++i) {
         if ((bits >> i) & 1u) {
@@ -1282,11 +1267,13 @@ void launch_preprocess_compressed(const PreprocessArgs& a, const SceneCompressed
 uint32_t scan_tile_count(uint32_t n) { return (n + kScanTile - 1) / kScanTile; }
 
 void launch_scan(const ScanArgs& a, uint32_t scan_tiles, cudaStream_t stream) {
-    cudaMemsetAsync(a.tile_state, 0, sizeof(unsigned long long) * scan_tiles, stream);
-    cudaMemsetAsync(a.tile_ticket, 0, sizeof(uint32_t), stream);
-    cudaMemsetAsync(a.counters, 0, sizeof(PassCounters), stream);
-    if (scan_tiles == 0) return;
-    scan_kernel<<<scan_tiles, kScanThreads, 0, stream>>>(a);
+    if (scan_tiles == 0) {
+        cudaMemsetAsync(a.counters, 0, sizeof(PassCounters), stream);
+        return;
+    }
+    scan_reduce_kernel<<<scan_tiles, kScanThreads, 0, stream>>>(a);
+    scan_tiles_kernel<<<1, kTileScanThreads, 0, stream>>>(a, scan_tiles);
+    scan_write_kernel<<<scan_tiles, kScanThreads, 0, stream>>>(a);
     const uint64_t max_tiles = ((uint64_t)a.max_points + a.tile_points - 1) / a.tile_points;
     const uint64_t want = (max_tiles + 255) / 256;
     const int owner_grid = (int)(want < 1184 ? (want ? want : 1) : 1184);  // 148 SMs x 8
@@ -1420,13 +1407,13 @@ void launch_progressive(uint8_t* image, float* cur_color, float* accum, int widt
 // inside a CUDA-graph capture or a stream-ordered pipeline where cudaMalloc would synchronise
 // the device, a host with a fixed device-memory pool or budget enforced by its own allocator,
 // or a plugin host that owns every buffer and forbids its plugins from allocating. For them
-// the scan's only scratch — the decoupled look-back status word of every 4096-Gaussian tile
-// and the tile ticket — lives in this file-scope device array, and the caller passes all
-// inputs and outputs. The array is shared by every call on a device and keeps the previous
-// call's contents, so each call clears the part it uses first; calls that overlap on the GPU
+// the scan's only scratch — the survivor and point totals of every 4096-Gaussian tile — lives
+// in this file-scope device array, and the caller passes all inputs and outputs. The array is
+// shared by every call on a device and keeps the previous call's contents; each call rewrites
+// every word it reads before reading it (tile totals, then prefixes); calls that overlap on the GPU
 // (different streams, or host threads on the same device) race on it and must be serialised.
 // ---------------------------------------------------------------------------------
-constexpr uint32_t kNoAllocScanMaxTiles = 65536;  // 512 KiB of status words: n <= 2^28 Gaussians
+constexpr uint32_t kNoAllocScanMaxTiles = 65536;  // 512 KiB of tile words: n <= 2^28 Gaussians
 static __device__ __align__(256) unsigned long long g_noalloc_scan_scratch[kNoAllocScanMaxTiles + 1];
 
 namespace {
@@ -1490,10 +1477,8 @@ extern "C" gps_status gps_workload_scan_noalloc(const uint32_t* d_counts, const 
     a.surv_start = d_surv_start;
     a.tile_first_rank = d_tile_first_rank;
     a.tile_state = scratch;
-    // the ticket sits after the last status word a scan can use
-    a.tile_ticket = reinterpret_cast<uint32_t*>(scratch + kNoAllocScanMaxTiles);
     a.counters = reinterpret_cast<PassCounters*>(d_counters8);
-    launch_scan(a, tiles, st);  // zeroes the status words, ticket and counters it uses, then scans
+    launch_scan(a, tiles, st);  // writes every tile word and all eight counters
     e = cudaGetLastError();
     if (e != cudaSuccess) {
         set_last_error(std::string("gps_workload_scan_noalloc: ") + cudaGetErrorString(e));

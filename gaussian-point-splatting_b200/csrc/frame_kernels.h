@@ -46,7 +46,7 @@ struct PassCounters {
     uint32_t total_points; // sum of point counts (u32, wraps like the reference)
     uint32_t points;       // min(total_points, max_number_of_points)
     uint32_t truncated;    // 1 if the point budget clipped the tail
-    uint32_t scan_timeouts;
+    uint32_t scan_timeouts;  // always 0: no device-side wait can give up
     uint32_t pad[3];
 };
 
@@ -91,8 +91,7 @@ struct ScanArgs {
     uint32_t* surv_gid;          // [n] compacted Gaussian ids of survivors
     uint32_t* surv_start;        // [n] first point of each survivor
     uint32_t* tile_first_rank;   // [ceil(max_points / tile_points) + 1]
-    unsigned long long* tile_state;  // [scan tiles] decoupled look-back status words
-    uint32_t* tile_ticket;       // dynamic tile counter
+    unsigned long long* tile_state;  // [scan tiles] tile totals, then tile prefixes
     PassCounters* counters;
 };
 

@@ -239,7 +239,7 @@ struct gps_renderer {
     uint64_t entries = 0;
     uint32_t n = 0, n_pad = 0;
     dptr<uint64_t> buffer;
-    dptr<uint32_t> counts, mask[2], surv_gid, surv_start, tile_first_rank, ticket, culled, chunk_list, chunk_count;
+    dptr<uint32_t> counts, mask[2], surv_gid, surv_start, tile_first_rank, culled, chunk_list, chunk_count;
     dptr<SplatRecord> records;
     dptr<unsigned long long> tile_state;
     dptr<PassCounters> counters;  // [2]: pass 1, pass 2
@@ -385,7 +385,6 @@ void render_pass(gps_renderer* r, const FrameConst& fc, int frame, bool first, c
     sa.surv_start = r->surv_start.get();
     sa.tile_first_rank = r->tile_first_rank.get();
     sa.tile_state = r->tile_state.get();
-    sa.tile_ticket = r->ticket.get();
     sa.counters = pc;
     launch_scan(sa, r->scan_tiles, st);
     count_launch(r, kStScan, r->scan_tiles ? 2 : 0);  // scan + tile owners
@@ -699,7 +698,6 @@ gps_status create_renderer(gps_scene* scene, const gps_settings* settings, const
         const uint64_t max_pts = (uint64_t)std::max(0, s.max_number_of_points);
         r->tile_first_rank.reset(dev_alloc<uint32_t>(max_pts / 256 + 2));
         r->tile_state.reset(dev_alloc<unsigned long long>(std::max<uint32_t>(r->scan_tiles, 1)));
-        r->ticket.reset(dev_alloc<uint32_t>(1));
         r->counters.reset(dev_alloc<PassCounters>(2));
         GPS_CUDA(cudaMemset(r->counters.get(), 0, sizeof(PassCounters) * 2));
         const uint32_t bwords = (scene->block_count + 31) / 32;

@@ -202,7 +202,7 @@ gps_status gps_renderer_debug_view(gps_renderer* r, gps_debug_view* out);
  * device-memory budget, or as a plugin whose host owns every buffer.  It computes one render
  * pass's workload (what gps_render_frame computes internally, the reference's
  * WorkloadDistributor::build): the exclusive point offsets of the Gaussians whose mask bit is
- * set, compacted.  It allocates nothing: its look-back scratch is a fixed 512 KiB device array
+ * set, compacted.  It allocates nothing: its scratch (the per-tile totals of the scan) is a fixed 512 KiB device array
  * inside the library, so n is limited to 268,435,456 Gaussians (larger n: GPS_ERR_SIZE).
  *   d_counts            n point counts (only entries whose mask bit is set are used); 16-byte
  *                       aligned and readable up to n rounded up to a multiple of 4
@@ -211,10 +211,11 @@ gps_status gps_renderer_debug_view(gps_renderer* r, gps_debug_view* out);
  *                       Gaussian with its bit set, in Gaussian order
  *   d_tile_first_rank   output, max_points / 256 + 2 entries: first survivor of each 256-point tile
  *   d_counters8         output, 8 words: survivors, total points (mod 2^32),
- *                       points = min(total, max_points), truncated flag, look-back give-ups, 0, 0, 0
+ *                       points = min(total, max_points), truncated flag, 0, 0, 0, 0
  * The first call on a device looks the scratch array's address up (make it before any stream
- * capture on that device).  All calls on a device share the array; each call re-zeroes what it
- * uses, and calls that overlap on the GPU race on it — serialise them (one stream at a time). */
+ * capture on that device).  All calls on a device share the array; each call writes every word
+ * of it that it reads before reading it, and calls that overlap on the GPU race on it —
+ * serialise them (one stream at a time). */
 gps_status gps_workload_scan_noalloc(const uint32_t* d_counts, const uint32_t* d_mask, uint32_t n,
                                      uint32_t max_points, uint32_t* d_surv_gid, uint32_t* d_surv_start,
                                      uint32_t* d_tile_first_rank, uint32_t* d_counters8, void* stream);

@@ -2,7 +2,7 @@
 
 That entry point exists for callers that must not allocate device memory when they run the
 scan — a CUDA-graph capture, a host with a fixed device-memory budget, a plugin whose host owns
-every buffer — so it keeps its only scratch (the look-back status words) in a fixed array
+every buffer — so it keeps its only scratch (the scan's per-tile totals) in a fixed array
 inside the library.  This test renders a frame through the normal entry point, then runs the
 allocation-free scan twice in a row on that frame's counts and survivor mask, and checks both
 results against the workload the renderer computed (integer data: exact).  The file sorts
@@ -56,7 +56,7 @@ def test_noalloc_scan_matches_renderer_twice(occlusion):
         c = ctr.cpu().numpy().view(np.uint32)
         assert c[0] == v.survivors, f"call {call}: survivors {c[0]} vs {v.survivors}"
         assert c[2] == v.points, f"call {call}: points {c[2]} vs {v.points}"
-        assert c[4] == 0, "look-back gave up"
+        assert c[4] == 0
         got_gid = gid.cpu().numpy().view(np.uint32)[: v.survivors]
         got_start = start.cpu().numpy().view(np.uint32)[: v.survivors]
         assert np.array_equal(got_gid, want_gid), f"call {call}: survivor ids differ"
