@@ -387,7 +387,7 @@ void render_pass(gps_renderer* r, const FrameConst& fc, int frame, bool first, c
     sa.tile_state = r->tile_state.get();
     sa.counters = pc;
     launch_scan(sa, r->scan_tiles, st);
-    count_launch(r, kStScan, r->scan_tiles ? 2 : 0);  // scan + tile owners
+    count_launch(r, kStScan, r->scan_tiles ? 4 : 0);  // tile reduce, tile scan, downsweep, tile owners
     r->timer.mark(kStSplat, st);
     SplatArgs sp{};
     sp.fc = fc;
