@@ -371,30 +371,48 @@ __global__ void __launch_bounds__(kScanThreads) scan_reduce_kernel(ScanArgs a) {
 }
 
 // Pass 2: one block turns the tile totals into exclusive tile prefixes (in place) and writes
-// the pass counters (points mod 2^32, like the reference's u32 offsets).
+// the pass counters (points mod 2^32, like the reference's u32 offsets).  The tile words go
+// through shared memory in rounds of kTileScanThreads * 4 with coalesced loads and stores;
+// each thread scans 4 consecutive words and a block scan plus a running carry joins them.
 constexpr int kTileScanThreads = 1024;
+constexpr int kTileScanPer = 4;
 __global__ void __launch_bounds__(kTileScanThreads) scan_tiles_kernel(ScanArgs a, uint32_t num_tiles) {
-    const uint32_t per = (num_tiles + kTileScanThreads - 1) / kTileScanThreads;
-    const uint32_t t0 = min(threadIdx.x * per, num_tiles), t1 = min(t0 + per, num_tiles);
-    uint32_t s = 0, p = 0;
-    for (uint32_t t = t0; t < t1; ++t) {
-        const unsigned long long v = a.tile_state[t];
-        s += (uint32_t)(v >> 32);
-        p += (uint32_t)v;
-    }
-    uint32_t ex_s, ex_p, tot_s, tot_p;
-    block_scan_pair<kTileScanThreads>(s, p, ex_s, ex_p, tot_s, tot_p);
-    for (uint32_t t = t0; t < t1; ++t) {
-        const unsigned long long v = a.tile_state[t];
-        a.tile_state[t] = ((unsigned long long)ex_s << 32) | ex_p;
-        ex_s += (uint32_t)(v >> 32);
-        ex_p += (uint32_t)v;
+    __shared__ unsigned long long words[kTileScanThreads * kTileScanPer];
+    constexpr uint32_t kRound = kTileScanThreads * kTileScanPer;
+    uint32_t carry_s = 0, carry_p = 0;
+    for (uint32_t r0 = 0; r0 < num_tiles; r0 += kRound) {
+        for (uint32_t i = threadIdx.x; i < kRound; i += kTileScanThreads)
+            words[i] = r0 + i < num_tiles ? a.tile_state[r0 + i] : 0ull;
+        __syncthreads();
+        uint32_t s = 0, p = 0;
+#pragma unroll
+        for (int k = 0; k < kTileScanPer; ++k) {
+            const unsigned long long v = words[threadIdx.x * kTileScanPer + k];
+            s += (uint32_t)(v >> 32);
+            p += (uint32_t)v;
+        }
+        uint32_t ex_s, ex_p, tot_s, tot_p;
+        block_scan_pair<kTileScanThreads>(s, p, ex_s, ex_p, tot_s, tot_p);
+        ex_s += carry_s;
+        ex_p += carry_p;
+#pragma unroll
+        for (int k = 0; k < kTileScanPer; ++k) {
+            const unsigned long long v = words[threadIdx.x * kTileScanPer + k];
+            words[threadIdx.x * kTileScanPer + k] = ((unsigned long long)ex_s << 32) | ex_p;
+            ex_s += (uint32_t)(v >> 32);
+            ex_p += (uint32_t)v;
+        }
+        __syncthreads();
+        for (uint32_t i = threadIdx.x; i < kRound && r0 + i < num_tiles; i += kTileScanThreads) a.tile_state[r0 + i] = words[i];
+        carry_s += tot_s;
+        carry_p += tot_p;
+        __syncthreads();
     }
     if (threadIdx.x == 0) {
-        a.counters->survivors = tot_s;
-        a.counters->total_points = tot_p;
-        a.counters->points = tot_p < a.max_points ? tot_p : a.max_points;
-        a.counters->truncated = tot_p > a.max_points ? 1u : 0u;
+        a.counters->survivors = carry_s;
+        a.counters->total_points = carry_p;
+        a.counters->points = carry_p < a.max_points ? carry_p : a.max_points;
+        a.counters->truncated = carry_p > a.max_points ? 1u : 0u;
         a.counters->scan_timeouts = 0u;
         a.counters->pad[0] = a.counters->pad[1] = a.counters->pad[2] = 0u;
     }
