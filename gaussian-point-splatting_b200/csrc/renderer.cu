@@ -9,6 +9,10 @@
 // a fixed sequence of asynchronous launches on the caller's stream.
 #include <algorithm>
 #include <cstdio>
+#include <thread>
+#include <deque>
+#include <condition_variable>
+#include <chrono>
 #include <cstring>
 #include <memory>
 #include <mutex>
@@ -249,6 +253,8 @@ struct gps_renderer {
     uint32_t scan_tiles = 0;
     uint64_t cap_entries = 0;     // splat-buffer and Hi-Z capacity (a batch worker renders
     uint64_t cap_mip = 0;         // views of different sizes within these)
+    uint32_t cap_n = 0;           // per-Gaussian scratch capacity (a server worker renders any
+    uint32_t cap_blocks = 0;      // resident scene up to these sizes)
     uint32_t iteration = 0;
     int splat_grid = 0;
     PassCounters* host_counters = nullptr;  // pinned [2]
@@ -654,9 +660,10 @@ gps_status configure_view(gps_renderer* r, int32_t width, int32_t height, int32_
     return GPS_OK;
 }
 
-// A renderer for `settings` whose splat buffer and Hi-Z also fit views of `capacity`'s size.
+// A renderer for `settings` whose splat buffer and Hi-Z also fit views of `capacity`'s size and
+// whose per-Gaussian scratch also fits scenes of up to cap_n Gaussians in cap_blocks blocks.
 gps_status create_renderer(gps_scene* scene, const gps_settings* settings, const gps_settings* capacity,
-                           gps_renderer** out) {
+                           gps_renderer** out, uint64_t cap_n = 0, uint32_t cap_blocks = 0) {
     if (!scene || !settings || !capacity || !out) return fail(GPS_ERR_INVALID_ARGUMENT, "null argument");
     *out = nullptr;
     const gps_settings& s = *settings;
@@ -679,7 +686,9 @@ gps_status create_renderer(gps_scene* scene, const gps_settings* settings, const
     r->up_w = (int)up_w;
     r->up_h = (int)up_h;
     r->entries = entries;
-    r->n = (uint32_t)scene->n;
+    r->cap_n = (uint32_t)std::max<uint64_t>(scene->n, cap_n);
+    r->cap_blocks = std::max<uint32_t>(scene->block_count, cap_blocks);
+    r->n = r->cap_n;  // size the per-Gaussian arrays for the capacity, then bind the scene
     r->scan_tiles = scan_tile_count(r->n);
     r->n_pad = r->scan_tiles * 4096;
     r->cap_entries = std::max(entries, cap_entries);
@@ -700,7 +709,7 @@ gps_status create_renderer(gps_scene* scene, const gps_settings* settings, const
         r->tile_state.reset(dev_alloc<unsigned long long>(std::max<uint32_t>(r->scan_tiles, 1)));
         r->counters.reset(dev_alloc<PassCounters>(2));
         GPS_CUDA(cudaMemset(r->counters.get(), 0, sizeof(PassCounters) * 2));
-        const uint32_t bwords = (scene->block_count + 31) / 32;
+        const uint32_t bwords = (r->cap_blocks + 31) / 32;
         r->culled.reset(dev_alloc<uint32_t>(bwords + 1));
         r->chunk_list.reset(dev_alloc<uint32_t>(words + 1));
         r->chunk_count.reset(dev_alloc<uint32_t>(1));
@@ -725,7 +734,21 @@ gps_status create_renderer(gps_scene* scene, const gps_settings* settings, const
     } catch (const CudaError& e) {
         return fail(std::string(e.what()).find("cudaMalloc") != std::string::npos ? GPS_ERR_OUT_OF_MEMORY : GPS_ERR_CUDA, e.what());
     }
+    r->n = (uint32_t)scene->n;
+    r->scan_tiles = scan_tile_count(r->n);
+    r->n_pad = r->scan_tiles * 4096;
     *out = r.release();
+    return GPS_OK;
+}
+
+// Points r at another resident scene whose sizes fit its per-Gaussian scratch.
+gps_status bind_scene(gps_renderer* r, gps_scene* scene) {
+    if (scene->n > r->cap_n || scene->block_count > r->cap_blocks)
+        return fail(GPS_ERR_SIZE, "scene larger than the renderer's per-Gaussian capacity");
+    r->scene = scene;
+    r->n = (uint32_t)scene->n;
+    r->scan_tiles = scan_tile_count(r->n);
+    r->n_pad = r->scan_tiles * 4096;
     return GPS_OK;
 }
 
@@ -1084,6 +1107,210 @@ gps_status gps_batch_autotune(gps_batch* b, const gps_view* views, int32_t count
     if (ms) *ms = best_ms;
     return rc;
 }
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------------
+// serving: request queue, dispatcher thread, GPU workers
+// ---------------------------------------------------------------------------------
+struct gps_server {
+    using clock = std::chrono::steady_clock;
+    struct Pending {
+        gps_request req;
+        clock::time_point submitted;
+    };
+    struct Worker {
+        gps_renderer* r = nullptr;
+        cudaStream_t st = nullptr;
+        cudaEvent_t ev = nullptr;
+        dptr<float> img, dep;          // outputs of requests that bring none
+        bool busy = false;
+        Pending job{};
+        clock::time_point admitted;
+    };
+    std::vector<gps_scene*> scenes;
+    std::vector<Worker> workers;
+    int device = 0;
+    std::mutex mu;
+    std::condition_variable cv;
+    std::deque<Pending> queue;
+    std::deque<gps_completion> done;
+    uint64_t submitted = 0, completed = 0;
+    bool stop = false;
+    std::thread dispatcher;
+    ~gps_server() {
+        {
+            std::lock_guard<std::mutex> lk(mu);
+            stop = true;
+        }
+        cv.notify_all();
+        if (dispatcher.joinable()) dispatcher.join();
+        cudaDeviceSynchronize();
+        for (Worker& w : workers) {
+            delete w.r;
+            if (w.st) cudaStreamDestroy(w.st);
+            if (w.ev) cudaEventDestroy(w.ev);
+        }
+    }
+};
+
+namespace {
+
+double ms_between(gps_server::clock::time_point a, gps_server::clock::time_point b) {
+    return std::chrono::duration<double, std::milli>(b - a).count();
+}
+
+// Called with the lock held.
+void finish(gps_server* sv, const gps_server::Pending& p, int worker, gps_status st,
+            gps_server::clock::time_point admitted) {
+    const auto now = gps_server::clock::now();
+    sv->done.push_back(gps_completion{p.req.id, (int32_t)st, worker, ms_between(p.submitted, admitted),
+                                      ms_between(p.submitted, now)});
+    ++sv->completed;
+    sv->cv.notify_all();
+}
+
+gps_status start_request(gps_server* sv, gps_server::Worker& w, const gps_request& q) {
+    if (q.scene < 0 || q.scene >= (int32_t)sv->scenes.size()) return fail(GPS_ERR_INVALID_ARGUMENT, "no such scene");
+    gps_status rc = bind_scene(w.r, sv->scenes[q.scene]);
+    if (rc != GPS_OK) return rc;
+    gps_view v{};
+    v.camera = q.camera;
+    v.width = q.width;
+    v.height = q.height;
+    v.samples_per_pixel = q.samples_per_pixel;
+    v.d_image = q.d_image ? q.d_image : w.img.get();
+    v.d_depth = q.d_depth ? q.d_depth : w.dep.get();
+    rc = render_view(w.r, v, w.st);
+    if (rc != GPS_OK) return rc;
+    cudaEventRecord(w.ev, w.st);
+    cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? GPS_OK : fail(GPS_ERR_CUDA, cudaGetErrorString(e));
+}
+
+void dispatch_loop(gps_server* sv) {
+    cudaSetDevice(sv->device);
+    std::unique_lock<std::mutex> lk(sv->mu);
+    for (;;) {
+        bool progressed = false, busy = false;
+        for (size_t i = 0; i < sv->workers.size(); ++i) {
+            gps_server::Worker& w = sv->workers[i];
+            if (!w.busy) continue;
+            const cudaError_t q = cudaEventQuery(w.ev);
+            if (q == cudaErrorNotReady) {
+                busy = true;
+                continue;
+            }
+            finish(sv, w.job, (int)i, q == cudaSuccess ? GPS_OK : GPS_ERR_CUDA, w.admitted);
+            w.busy = false;
+            progressed = true;
+        }
+        for (size_t i = 0; i < sv->workers.size() && !sv->queue.empty(); ++i) {
+            gps_server::Worker& w = sv->workers[i];
+            if (w.busy) continue;
+            gps_server::Pending p = sv->queue.front();
+            sv->queue.pop_front();
+            lk.unlock();  // launch without blocking submitters
+            const auto admitted = gps_server::clock::now();
+            const gps_status rc = start_request(sv, w, p.req);
+            lk.lock();
+            if (rc == GPS_OK) {
+                w.busy = true;
+                w.job = p;
+                w.admitted = admitted;
+                busy = true;
+            } else {
+                finish(sv, p, (int)i, rc, admitted);
+            }
+            progressed = true;
+        }
+        if (sv->stop && sv->queue.empty() && !busy) break;
+        if (progressed) continue;
+        if (busy) {  // poll the workers' events again shortly
+            lk.unlock();
+            std::this_thread::sleep_for(std::chrono::microseconds(20));
+            lk.lock();
+        } else {
+            sv->cv.wait_for(lk, std::chrono::milliseconds(5), [&] { return sv->stop || !sv->queue.empty(); });
+        }
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+gps_status gps_server_create(gps_scene* const* scenes, int32_t n_scenes, const gps_settings* settings,
+                             int32_t max_width, int32_t max_height, int32_t max_spp, int32_t workers,
+                             gps_server** out) {
+    if (!scenes || n_scenes < 1 || !settings || !out) return fail(GPS_ERR_INVALID_ARGUMENT, "null argument");
+    *out = nullptr;
+    if (workers < 1 || workers > 64) return fail(GPS_ERR_INVALID_ARGUMENT, "workers must be 1..64");
+    auto sv = std::make_unique<gps_server>();
+    uint64_t cap_n = 0;
+    uint32_t cap_blocks = 0;
+    for (int i = 0; i < n_scenes; ++i) {
+        if (!scenes[i]) return fail(GPS_ERR_INVALID_ARGUMENT, "null scene");
+        sv->scenes.push_back(scenes[i]);
+        cap_n = std::max<uint64_t>(cap_n, scenes[i]->n);
+        cap_blocks = std::max(cap_blocks, scenes[i]->block_count);
+    }
+    cudaGetDevice(&sv->device);
+    gps_settings cap = *settings;
+    cap.width = max_width;
+    cap.height = max_height;
+    cap.samples_per_pixel = max_spp;
+    sv->workers.resize(workers);
+    for (gps_server::Worker& w : sv->workers) {
+        gps_status rc = create_renderer(scenes[0], &cap, &cap, &w.r, cap_n, cap_blocks);
+        if (rc != GPS_OK) return rc;
+        try {
+            w.img.reset(dev_alloc<float>((size_t)max_width * max_height * 3));
+            w.dep.reset(dev_alloc<float>((size_t)max_width * max_height));
+        } catch (const CudaError& e) {
+            return fail(GPS_ERR_OUT_OF_MEMORY, e.what());
+        }
+        if (cudaStreamCreateWithFlags(&w.st, cudaStreamNonBlocking) != cudaSuccess ||
+            cudaEventCreateWithFlags(&w.ev, cudaEventDisableTiming) != cudaSuccess)
+            return fail(GPS_ERR_CUDA, "stream or event creation failed");
+    }
+    gps_server* raw = sv.get();
+    raw->dispatcher = std::thread(dispatch_loop, raw);
+    *out = sv.release();
+    return GPS_OK;
+}
+
+gps_status gps_server_submit(gps_server* s, const gps_request* req) {
+    if (!s || !req) return fail(GPS_ERR_INVALID_ARGUMENT, "null argument");
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        s->queue.push_back(gps_server::Pending{*req, gps_server::clock::now()});
+        ++s->submitted;
+    }
+    s->cv.notify_all();
+    return GPS_OK;
+}
+
+int32_t gps_server_poll(gps_server* s, gps_completion* out, int32_t capacity) {
+    if (!s || !out || capacity <= 0) return 0;
+    std::lock_guard<std::mutex> lk(s->mu);
+    int32_t n = 0;
+    while (n < capacity && !s->done.empty()) {
+        out[n++] = s->done.front();
+        s->done.pop_front();
+    }
+    return n;
+}
+
+gps_status gps_server_drain(gps_server* s, double timeout_s) {
+    if (!s) return fail(GPS_ERR_INVALID_ARGUMENT, "null argument");
+    std::unique_lock<std::mutex> lk(s->mu);
+    const bool ok = s->cv.wait_for(lk, std::chrono::duration<double>(timeout_s),
+                                   [&] { return s->completed == s->submitted; });
+    return ok ? GPS_OK : fail(GPS_ERR_DEVICE_TIMEOUT, "requests still in flight after the drain timeout");
+}
+
+void gps_server_free(gps_server* s) { delete s; }
 
 }  // extern "C"
 

@@ -88,6 +88,17 @@ class View(ctypes.Structure):
                 ("d_image", c_void_p), ("d_depth", c_void_p)]
 
 
+class Request(ctypes.Structure):
+    """gps_request: one render request for a server."""
+    _fields_ = [("id", c_uint64), ("scene", c_int32), ("camera", Camera), ("width", c_int32), ("height", c_int32),
+                ("samples_per_pixel", c_int32), ("d_image", c_void_p), ("d_depth", c_void_p)]
+
+
+class Completion(ctypes.Structure):
+    _fields_ = [("id", c_uint64), ("status", c_int32), ("worker", c_int32), ("queued_ms", ctypes.c_double),
+                ("latency_ms", ctypes.c_double)]
+
+
 class CameraState(ctypes.Structure):
     _fields_ = [
         ("id", c_int32),
@@ -170,6 +181,11 @@ _SIGNATURES = [
     ("gps_batch_set_workers", c_int32, [c_void_p, c_int32]),
     ("gps_batch_workers", c_int32, [c_void_p]),
     ("gps_batch_autotune", c_int32, [c_void_p, POINTER(View), c_int32, c_int32, c_void_p, POINTER(c_int32), POINTER(c_float)]),
+    ("gps_server_create", c_int32, [POINTER(c_void_p), c_int32, POINTER(Settings), c_int32, c_int32, c_int32, c_int32, POINTER(c_void_p)]),
+    ("gps_server_submit", c_int32, [c_void_p, POINTER(Request)]),
+    ("gps_server_poll", c_int32, [c_void_p, POINTER(Completion), c_int32]),
+    ("gps_server_drain", c_int32, [c_void_p, ctypes.c_double]),
+    ("gps_server_free", None, [c_void_p]),
     ("gps_frame_loop_create", c_int32, [c_void_p, POINTER(c_void_p)]),
     ("gps_frame_loop_free", None, [c_void_p]),
     ("gps_frame_loop_step", c_int32, [c_void_p, POINTER(Camera), c_void_p]),
@@ -457,6 +473,41 @@ class Batch:
     def close(self):
         if self._h:
             load_library().gps_batch_free(self._h)
+            self._h = c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Server:
+    """Request loop over resident scenes (gps_server_*): submit from any thread, poll completions."""
+
+    def __init__(self, scenes, settings: Settings, max_width: int, max_height: int, max_spp: int, workers: int = 4):
+        self.scenes = list(scenes)
+        arr = (c_void_p * len(self.scenes))(*[sc._h.value for sc in self.scenes])
+        self._h = c_void_p()
+        _check(load_library().gps_server_create(arr, len(self.scenes), byref(settings), max_width, max_height, max_spp,
+                                                workers, byref(self._h)))
+
+    def submit(self, req_id: int, scene: int, cam: Camera, width: int, height: int, spp: int,
+               d_image: int = 0, d_depth: int = 0):
+        q = Request(req_id, scene, cam, width, height, spp, c_void_p(d_image or None), c_void_p(d_depth or None))
+        _check(load_library().gps_server_submit(self._h, byref(q)))
+
+    def poll(self, capacity: int = 256):
+        buf = (Completion * capacity)()
+        n = load_library().gps_server_poll(self._h, buf, capacity)
+        return [(c.id, c.status, c.worker, c.queued_ms, c.latency_ms) for c in buf[:n]]
+
+    def drain(self, timeout_s: float = 600.0):
+        _check(load_library().gps_server_drain(self._h, timeout_s))
+
+    def close(self):
+        if self._h:
+            load_library().gps_server_free(self._h)
             self._h = c_void_p()
 
     def __del__(self):

@@ -252,6 +252,43 @@ int32_t gps_batch_workers(const gps_batch* b);
 gps_status gps_batch_autotune(gps_batch* b, const gps_view* views, int32_t count, int32_t rounds, void* stream,
                               int32_t* chosen, float* ms);
 
+/* ---- serving: a request loop over resident scenes -------------------------------------
+ * Render requests (scene, camera, resolution, spp) are submitted from any host thread and
+ * queued; a dispatcher thread of the server admits them, first come first served, onto
+ * `workers` GPU workers (each with its own stream, per-Gaussian scratch for the largest
+ * scene and a splat buffer for the largest view) as soon as a worker is free, so requests
+ * that arrive while others are on the GPU start as slots free up and their work overlaps on
+ * the device.  A request larger than the workers' capacity completes with GPS_ERR_SIZE.  Each
+ * request is rendered as a fresh renderer's first frame (like gps_batch_render), so its result
+ * does not depend on what else is in flight.  The device current at gps_server_create is used. */
+typedef struct gps_request {
+    uint64_t id;                 /* caller's tag, returned in the completion */
+    int32_t scene;               /* index into the scenes passed to gps_server_create */
+    gps_camera camera;
+    int32_t width, height, samples_per_pixel;
+    float* d_image;              /* width * height float3, or NULL to render into the worker's buffer */
+    float* d_depth;              /* width * height float, or NULL */
+} gps_request;
+typedef struct gps_completion {
+    uint64_t id;
+    int32_t status;              /* gps_status of this request */
+    int32_t worker;
+    double queued_ms;            /* submit -> admitted to a worker */
+    double latency_ms;           /* submit -> its GPU work seen finished */
+} gps_completion;
+typedef struct gps_server gps_server;
+gps_status gps_server_create(gps_scene* const* scenes, int32_t n_scenes, const gps_settings* settings,
+                             int32_t max_width, int32_t max_height, int32_t max_spp, int32_t workers,
+                             gps_server** out);
+/* Queues one request; thread-safe and never waits for the GPU. */
+gps_status gps_server_submit(gps_server* s, const gps_request* req);
+/* Moves up to `capacity` completions (oldest first) to `out`; returns how many. */
+int32_t gps_server_poll(gps_server* s, gps_completion* out, int32_t capacity);
+/* Waits until every submitted request has completed (GPS_ERR_DEVICE_TIMEOUT after timeout_s). */
+gps_status gps_server_drain(gps_server* s, double timeout_s);
+/* Drains, stops the dispatcher and frees the workers (the scenes stay the caller's). */
+void gps_server_free(gps_server* s);
+
 /* ---- RenderServer post-process (render_server.cu:122-157) ---------------------------- */
 /* temporalRender (post_processing_kernels.cuh:222-285): reprojects history through reproj
  * (column-major), clamps it to the 3x3 neighbourhood of the current colour +-0.05, blends,
