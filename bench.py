@@ -357,6 +357,98 @@ def run_batch_workload(args, world, rank, local):
 
 
 # ---------------------------------------------------------------------------------
+# serving workload: Poisson arrivals over the 16M FP32 and 256M half-precision towns
+# ---------------------------------------------------------------------------------
+SERVE_RES = [(640, 360), (1280, 720), (1920, 1080), (3840, 2160)]
+SERVE_SPP = [1, 4, 16]
+SERVE_RATES = [50.0, 200.0, 1000.0]
+
+
+def run_serve_workload(args, world, rank, local):
+    """Requests arrive as a Poisson process (SERVE_RATES req/s, `--steps` x 20 requests per
+    rate): 70% for the 16M town (FP32), 30% for the 256M town (half precision, 4 x 4 tiles),
+    seeded poses, resolution from SERVE_RES, spp from SERVE_SPP, supersampling 2, culling on.
+    The server (4 workers, continuous admission) is measured beside the plain loop (one worker,
+    one request at a time, same arrivals): served views/s and p50/p99 latency from submission
+    to the end of the request's GPU work."""
+    import torch
+
+    torch.cuda.set_device(local)
+    import gpsplat
+
+    gpsplat.load_library()
+    g_host = load_scene_host(workload_spec("town16m"))
+    town = gpsplat.Scene.from_host(np.ascontiguousarray(g_host), presorted=True)
+    half = gpsplat.Scene.from_host(np.ascontiguousarray(g_host), gpsplat.GPS_SCENE_HALF, presorted=True)
+    ext = synth.TOWN_EXTENT
+    big = half.tile([[(i - 1.5) * ext, (j - 1.5) * ext] for j in range(4) for i in range(4)])
+    half.close()
+    scenes = [town, big]
+    base = dict(supersampling_factor=2, enable_hierarchical_culling=1, enable_occlusion_culling=1)
+    n_req = max(20, args.steps * 20)
+    rng = np.random.default_rng(5 + rank)
+    poses = synth.random_poses(n_req, seed=21 + rank)
+    reqs = []
+    for i in range(n_req):
+        w, h = SERVE_RES[int(rng.integers(len(SERVE_RES)))]
+        spp = SERVE_SPP[int(rng.integers(len(SERVE_SPP)))]
+        s = gpsplat.default_settings(**base, width=w, height=h, samples_per_pixel=spp)
+        p, r = poses[i]
+        cam = gpsplat.camera_from_pose(p, np.asarray(r, np.float32).T, s, i + 1)
+        reqs.append((i, 0 if rng.random() < 0.7 else 1, cam, w, h, spp))
+    cap = gpsplat.default_settings(**base, width=3840, height=2160, samples_per_pixel=16)
+
+    def run(server, rate, seed):
+        gaps = np.random.default_rng(seed).exponential(1.0 / rate, size=len(reqs))
+        t0 = time.perf_counter()
+        due = t0
+        for q, gap in zip(reqs, gaps):
+            due += gap
+            delay = due - time.perf_counter()
+            if delay > 0:
+                time.sleep(delay)
+            server.submit(*q)
+        server.drain(1200.0)
+        wall = time.perf_counter() - t0
+        done = server.poll(len(reqs) + 8)
+        assert len(done) == len(reqs) and all(c[1] == 0 for c in done), "a request failed"
+        lat = np.array([c[4] for c in done])
+        return {"rate_req_s": rate, "views_per_s": len(reqs) / wall, "p50_ms": float(np.percentile(lat, 50)),
+                "p99_ms": float(np.percentile(lat, 99)), "workers_used": len({c[2] for c in done})}
+
+    results = {}
+    for mode, workers, budget in (("server", 4, None), ("server_unlimited", 4, 0), ("plain", 1, None)):
+        server = gpsplat.Server(scenes, cap, 3840, 2160, 16, workers=workers)
+        if budget is not None:
+            server.set_admission(budget)
+        for q in reqs[: min(8, len(reqs))]:  # warm-up
+            server.submit(*q)
+        server.drain(1200.0)
+        server.poll(64)
+        results[mode] = [run(server, rate, 100 + k) for k, rate in enumerate(SERVE_RATES)]
+        server.close()
+    top = results["server"][-1]
+    line = {
+        "metric": "served views/sec", "value": top["views_per_s"] * world, "unit": "views/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 / top["views_per_s"] * 20,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32 (16M town), f16/fp8 storage (256M town)",
+        "data": "synthetic (seeded towns, poses and Poisson arrivals, see synth.py)",
+        "config": {"workload": "serve", "requests_per_rate": len(reqs), "scenes": {"town16m_fp32": 0.7, "town256m_half": 0.3},
+                   "resolutions": SERVE_RES, "spp": SERVE_SPP, "supersampling": 2, "rates_req_s": SERVE_RATES,
+                   "server_workers": 4, "parallelism": f"replicas x{world}"},
+        "server": results["server"], "plain": results["plain"],
+        "speedup_vs_plain_at_top_rate": top["views_per_s"] / results["plain"][-1]["views_per_s"],
+        "e2e": {"value": top["views_per_s"] * world, "unit": "views/s", "h2d_bytes_per_step": 20 * 128,
+                "d2h_bytes_per_step": 0, "note": "requests handed over from host memory; images stay on the device"},
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    for sc in scenes:
+        sc.close()
+    return 0
+
+
+# ---------------------------------------------------------------------------------
 # the GPU arm
 # ---------------------------------------------------------------------------------
 def main():
@@ -365,7 +457,7 @@ def main():
     ap.add_argument("--steps", type=int, default=30)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="mine", choices=["mine", "reference"])
-    ap.add_argument("--workload", default="town16m", choices=["town16m", "town4m", "town256m", "cube1m", "batch64"])
+    ap.add_argument("--workload", default="town16m", choices=["town16m", "town4m", "town256m", "cube1m", "batch64", "serve"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
@@ -377,6 +469,13 @@ def main():
                                   "batch64 views/s comparison is against this library's plain single-view path"}))
             return 0
         return run_batch_workload(args, world, rank, local)
+    if args.workload == "serve":
+        if args.impl == "reference":
+            if rank == 0:
+                print(json.dumps({"impl": "reference", "unavailable": "the reference has no request server; the "
+                                  "serve comparison is against this library's one-request-at-a-time loop"}))
+            return 0
+        return run_serve_workload(args, world, rank, local)
     spec = workload_spec(args.workload)
     if args.impl == "reference":
         return run_reference_arm(args, spec, world, rank)

@@ -1126,6 +1126,7 @@ struct gps_server {
         dptr<float> img, dep;          // outputs of requests that bring none
         bool busy = false;
         Pending job{};
+        uint64_t entries = 0;          // splat-buffer entries of the request in flight
         clock::time_point admitted;
     };
     std::vector<gps_scene*> scenes;
@@ -1136,6 +1137,9 @@ struct gps_server {
     std::deque<Pending> queue;
     std::deque<gps_completion> done;
     uint64_t submitted = 0, completed = 0;
+    uint64_t max_inflight = 67108864ull;   // admission budget in splat-buffer entries (0 = none)
+    uint64_t inflight = 0;
+    int ss = 1;
     bool stop = false;
     std::thread dispatcher;
     ~gps_server() {
@@ -1203,11 +1207,17 @@ void dispatch_loop(gps_server* sv) {
             }
             finish(sv, w.job, (int)i, q == cudaSuccess ? GPS_OK : GPS_ERR_CUDA, w.admitted);
             w.busy = false;
+            sv->inflight -= w.entries;
             progressed = true;
         }
         for (size_t i = 0; i < sv->workers.size() && !sv->queue.empty(); ++i) {
             gps_server::Worker& w = sv->workers[i];
             if (w.busy) continue;
+            const gps_request& head = sv->queue.front().req;
+            const uint64_t need = head.width > 0 && head.height > 0 && head.samples_per_pixel > 0
+                                      ? splat_buffer_entries(head.width * sv->ss, head.height * sv->ss, head.samples_per_pixel)
+                                      : 0;
+            if (sv->inflight > 0 && sv->max_inflight > 0 && sv->inflight + need > sv->max_inflight) break;  // FIFO: wait
             gps_server::Pending p = sv->queue.front();
             sv->queue.pop_front();
             lk.unlock();  // launch without blocking submitters
@@ -1218,6 +1228,8 @@ void dispatch_loop(gps_server* sv) {
                 w.busy = true;
                 w.job = p;
                 w.admitted = admitted;
+                w.entries = need;
+                sv->inflight += need;
                 busy = true;
             } else {
                 finish(sv, p, (int)i, rc, admitted);
@@ -1256,6 +1268,7 @@ gps_status gps_server_create(gps_scene* const* scenes, int32_t n_scenes, const g
         cap_blocks = std::max(cap_blocks, scenes[i]->block_count);
     }
     cudaGetDevice(&sv->device);
+    sv->ss = settings->supersampling_factor > 0 ? settings->supersampling_factor : 1;
     gps_settings cap = *settings;
     cap.width = max_width;
     cap.height = max_height;
@@ -1277,6 +1290,13 @@ gps_status gps_server_create(gps_scene* const* scenes, int32_t n_scenes, const g
     gps_server* raw = sv.get();
     raw->dispatcher = std::thread(dispatch_loop, raw);
     *out = sv.release();
+    return GPS_OK;
+}
+
+gps_status gps_server_set_admission(gps_server* s, uint64_t max_inflight_entries) {
+    if (!s) return fail(GPS_ERR_INVALID_ARGUMENT, "null argument");
+    std::lock_guard<std::mutex> lk(s->mu);
+    s->max_inflight = max_inflight_entries;
     return GPS_OK;
 }
 

@@ -182,6 +182,7 @@ _SIGNATURES = [
     ("gps_batch_workers", c_int32, [c_void_p]),
     ("gps_batch_autotune", c_int32, [c_void_p, POINTER(View), c_int32, c_int32, c_void_p, POINTER(c_int32), POINTER(c_float)]),
     ("gps_server_create", c_int32, [POINTER(c_void_p), c_int32, POINTER(Settings), c_int32, c_int32, c_int32, c_int32, POINTER(c_void_p)]),
+    ("gps_server_set_admission", c_int32, [c_void_p, c_uint64]),
     ("gps_server_submit", c_int32, [c_void_p, POINTER(Request)]),
     ("gps_server_poll", c_int32, [c_void_p, POINTER(Completion), c_int32]),
     ("gps_server_drain", c_int32, [c_void_p, ctypes.c_double]),
@@ -496,6 +497,10 @@ class Server:
                d_image: int = 0, d_depth: int = 0):
         q = Request(req_id, scene, cam, width, height, spp, c_void_p(d_image or None), c_void_p(d_depth or None))
         _check(load_library().gps_server_submit(self._h, byref(q)))
+
+    def set_admission(self, max_inflight_entries: int):
+        """Splat-buffer entries allowed in flight at once (0 = no limit)."""
+        _check(load_library().gps_server_set_admission(self._h, max_inflight_entries))
 
     def poll(self, capacity: int = 256):
         buf = (Completion * capacity)()

@@ -280,6 +280,12 @@ typedef struct gps_server gps_server;
 gps_status gps_server_create(gps_scene* const* scenes, int32_t n_scenes, const gps_settings* settings,
                              int32_t max_width, int32_t max_height, int32_t max_spp, int32_t workers,
                              gps_server** out);
+/* Admission budget: a request joins the requests in flight only while their splat buffers
+ * together hold at most `max_inflight_entries` entries (W*ss x H*ss x spp, rounded up to 64x64
+ * tiles); a request above the budget runs alone.  Large views saturate the GPU by themselves
+ * and only slow each other down when overlapped, small ones fill it together.  0 = no limit.
+ * Default: 67,108,864 entries (two 1920x1080 views at ss 2 and 4 spp). */
+gps_status gps_server_set_admission(gps_server* s, uint64_t max_inflight_entries);
 /* Queues one request; thread-safe and never waits for the GPU. */
 gps_status gps_server_submit(gps_server* s, const gps_request* req);
 /* Moves up to `capacity` completions (oldest first) to `out`; returns how many. */
