@@ -436,7 +436,7 @@ def run_serve_workload(args, world, rank, local):
         "config": {"workload": "serve", "requests_per_rate": len(reqs), "scenes": {"town16m_fp32": 0.7, "town256m_half": 0.3},
                    "resolutions": SERVE_RES, "spp": SERVE_SPP, "supersampling": 2, "rates_req_s": SERVE_RATES,
                    "server_workers": 4, "parallelism": f"replicas x{world}"},
-        "server": results["server"], "plain": results["plain"],
+        "server": results["server"], "server_no_admission_budget": results["server_unlimited"], "plain": results["plain"],
         "speedup_vs_plain_at_top_rate": top["views_per_s"] / results["plain"][-1]["views_per_s"],
         "e2e": {"value": top["views_per_s"] * world, "unit": "views/s", "h2d_bytes_per_step": 20 * 128,
                 "d2h_bytes_per_step": 0, "note": "requests handed over from host memory; images stay on the device"},
