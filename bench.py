@@ -189,6 +189,22 @@ def barrier(world: int):
 # ---------------------------------------------------------------------------------
 # CPU baseline (the oracle, oracle/oracle.cpp) on a bounded sample of the workload
 # ---------------------------------------------------------------------------------
+def measured_traffic(kernel: str, spec):
+    """DRAM bytes per splat launch from the committed ncu summary (dram__bytes_read.sum +
+    dram__bytes_write.sum, averaged over a frame's two launches).  The splat's traffic follows
+    its buffer (1080p, ss 2, 4 spp for every town workload), not the Gaussian count."""
+    if kernel != "splat" or spec.get("kind") != "town" or (spec["width"], spec["height"], spec["ss"], spec["spp"]) != (1920, 1080, 2, 4):
+        return None
+    try:
+        with open(os.path.join(ROOT, "profiles", "kernels_town4m_1080p_ss2_spp4_full.md")) as f:
+            for ln in f:
+                if ln.startswith("traffic_per_launch_bytes:"):
+                    return float(ln.split(":")[1])
+    except OSError:
+        pass
+    return None
+
+
 def cpu_baseline(gpsplat, g_host, spec, settings, poses, budget_s: float = 12.0):
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle
@@ -593,9 +609,12 @@ def main():
     else:
         alg_bytes = 8.0 * entries
     achieved = alg_bytes / (per_launch_ms / 1000.0) / 1e9
+    traffic = measured_traffic(dom, spec)
     roofline = {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
-                "frac": achieved / hbm_peak, "traffic": None, "peak_source": peak_src,
-                "algorithmic_bytes_per_launch": alg_bytes, "ms_per_launch": per_launch_ms}
+                "frac": achieved / hbm_peak, "traffic": traffic, "peak_source": peak_src,
+                "algorithmic_bytes_per_launch": alg_bytes, "ms_per_launch": per_launch_ms,
+                "traffic_source": "profiles/kernels_town4m_1080p_ss2_spp4_full.md (ncu dram bytes of the same "
+                                  "1080p ss 2, 4 spp splat buffer)" if traffic else None}
 
     line = {
         "metric": "Gaussians/sec", "value": value, "unit": "Gaussians/s", "n_gpus": world, "steps": K,
