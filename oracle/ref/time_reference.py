@@ -36,6 +36,8 @@ def main():
     ap.add_argument("--frames", type=int, default=30)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--variant", default="fp32", choices=["fp32", "compressed"])
+    ap.add_argument("--workload", default="town", choices=["town", "cube"],
+                    help="town: 1080p ss 2, 4 spp, culling, TAA, orbit; cube: 640x360 ss 1, 1 spp, no culling, static camera")
     args = ap.parse_args()
     import torch
 
@@ -43,14 +45,21 @@ def main():
     if exe is None:
         raise SystemExit("reference harness not built (oracle/ref/build_ref.sh)")
     work = tempfile.mkdtemp(prefix="gps_time_ref_")
-    ply = os.path.join(work, f"town{args.n}.ply")
+    ply = os.path.join(work, f"{args.workload}{args.n}.ply")
     t = time.time()
-    synth.town(args.n).write_ply(ply)
+    (synth.town(args.n) if args.workload == "town" else synth.cube(args.n)).write_ply(ply)
     print(f"scene written in {time.time() - t:.1f}s", file=sys.stderr)
-    s = gpsplat.default_settings(width=1920, height=1080, supersampling_factor=2, samples_per_pixel=4,
-                                 accumulation_mode=gpsplat.GPS_ACCUM_TAA)
     total = args.warmup + args.frames
-    cams = gpsutil.cameras_for(s, synth.orbit(120, 30.0, 10.0)[:total])
+    if args.workload == "town":
+        s = gpsplat.default_settings(width=1920, height=1080, supersampling_factor=2, samples_per_pixel=4,
+                                     accumulation_mode=gpsplat.GPS_ACCUM_TAA)
+        cams = gpsutil.cameras_for(s, synth.orbit(120, 30.0, 10.0)[:total])
+    else:
+        s = gpsplat.default_settings(width=640, height=360, supersampling_factor=1, samples_per_pixel=1,
+                                     fully_disable_hierarchical_culling=1, enable_occlusion_culling=0,
+                                     accumulation_mode=gpsplat.GPS_ACCUM_NONE)
+        p = np.array([0.0, 0.0, -30.0])
+        cams = gpsutil.cameras_for(s, [(p, synth.look_at_c2w(p, [0.0, 0.0, 0.0]))] * total)
     camf = os.path.join(work, "cams.bin")
     gpsutil.write_camera_file(camf, cams)
     res = subprocess.run([exe, "render", ply, work, camf] + gpsutil.harness_args(s) +
@@ -76,8 +85,9 @@ def main():
         e1.record()
         e1.synchronize()
         ms.append(e0.elapsed_time(e1))
-    out = {"gaussians": args.n, "format": args.variant, "frames": args.frames, "resolution": [1920, 1080],
-           "supersampling": 2, "spp": 4, "culling": True, "taa": True,
+    out = {"workload": args.workload, "gaussians": args.n, "format": args.variant, "frames": args.frames,
+           "resolution": [s.width, s.height], "supersampling": s.supersampling_factor, "spp": s.samples_per_pixel,
+           "culling": bool(s.enable_occlusion_culling), "taa": s.accumulation_mode == gpsplat.GPS_ACCUM_TAA,
            "reference_ms_per_frame": ref["ms_per_frame"], "this_ms_per_frame": float(np.mean(ms)),
            "speedup": ref["ms_per_frame"] / float(np.mean(ms))}
     print(json.dumps(out))
