@@ -25,8 +25,9 @@ namespace gps {
 namespace {
 
 constexpr int kScanThreads = 256;
-constexpr int kScanItems = 16;
-constexpr uint32_t kScanTile = kScanThreads * kScanItems;  // 4096 Gaussians per scan tile
+constexpr int kScanItems = 16;   // per thread and round
+constexpr int kScanRounds = 4;   // a thread covers kScanItems * kScanRounds consecutive Gaussians
+constexpr uint32_t kScanTile = kScanThreads * kScanItems * kScanRounds;  // 16384 Gaussians per scan tile
 
 // ---------------------------------------------------------------------------------
 // Hi-Z query (depth_mip_chain.cuh:172-215, the non-tree variant the reference compiles)
@@ -301,7 +302,7 @@ __global__ void __launch_bounds__(256) preprocess_kernel(PreprocessArgs a, Scene
 // the reference's u32 offsets).  No block waits on another, so there is no spin at all.
 // ---------------------------------------------------------------------------------
 
-// One scan tile (4096 Gaussians, 16 per thread): the thread's mask bits and point counts.
+// One round of a thread's Gaussians (16 consecutive): its mask bits and point counts.
 __device__ __forceinline__ uint32_t scan_load(const ScanArgs& a, uint32_t base, uint32_t cnt[kScanItems]) {
     uint32_t bits = 0;
     if (base < a.n) {
@@ -360,13 +361,17 @@ __device__ __forceinline__ void block_scan_pair(uint32_t s, uint32_t p, uint32_t
 // Pass 1 of the scan: every tile's survivor and point totals, fully parallel.
 __global__ void __launch_bounds__(kScanThreads) scan_reduce_kernel(ScanArgs a) {
     const uint32_t tile = blockIdx.x;
-    uint32_t cnt[kScanItems];
-    const uint32_t bits = scan_load(a, tile * kScanTile + threadIdx.x * kScanItems, cnt);
-    uint32_t pts = 0;
+    const uint32_t base = tile * kScanTile + threadIdx.x * (kScanItems * kScanRounds);
+    uint32_t surv = 0, pts = 0;
 #pragma unroll
-    for (int i = 0; i < kScanItems; ++i) pts += cnt[i];
+    for (int q = 0; q < kScanRounds; ++q) {
+        uint32_t cnt[kScanItems];
+        surv += __popc(scan_load(a, base + q * kScanItems, cnt));
+#pragma unroll
+        for (int i = 0; i < kScanItems; ++i) pts += cnt[i];
+    }
     uint32_t ex_s, ex_p, tot_s, tot_p;
-    block_scan_pair<kScanThreads>(__popc(bits), pts, ex_s, ex_p, tot_s, tot_p);
+    block_scan_pair<kScanThreads>(surv, pts, ex_s, ex_p, tot_s, tot_p);
     if (threadIdx.x == 0) a.tile_state[tile] = ((unsigned long long)tot_s << 32) | tot_p;
 }
 
@@ -422,25 +427,33 @@ __global__ void __launch_bounds__(kTileScanThreads) scan_tiles_kernel(ScanArgs a
 // ids and first points.
 __global__ void __launch_bounds__(kScanThreads) scan_write_kernel(ScanArgs a) {
     const uint32_t tile = blockIdx.x;
-    const uint32_t base = tile * kScanTile + threadIdx.x * kScanItems;
-    uint32_t cnt[kScanItems];
-    const uint32_t bits = scan_load(a, base, cnt);
-    uint32_t pts = 0;
+    const uint32_t base = tile * kScanTile + threadIdx.x * (kScanItems * kScanRounds);
+    uint32_t surv = 0, pts = 0;
 #pragma unroll
-    for (int i = 0; i < kScanItems; ++i) pts += cnt[i];
+    for (int q = 0; q < kScanRounds; ++q) {
+        uint32_t cnt[kScanItems];
+        surv += __popc(scan_load(a, base + q * kScanItems, cnt));
+#pragma unroll
+        for (int i = 0; i < kScanItems; ++i) pts += cnt[i];
+    }
     uint32_t ex_s, ex_p, tot_s, tot_p;
-    block_scan_pair<kScanThreads>(__popc(bits), pts, ex_s, ex_p, tot_s, tot_p);
-    if (bits == 0u) return;
+    block_scan_pair<kScanThreads>(surv, pts, ex_s, ex_p, tot_s, tot_p);
+    if (surv == 0u) return;
     const unsigned long long pre = a.tile_state[tile];
     uint32_t r = (uint32_t)(pre >> 32) + ex_s;
     uint32_t pt = (uint32_t)pre + ex_p;
+    for (int q = 0; q < kScanRounds; ++q) {  // again, now writing (the counts come from L1/L2)
+        uint32_t cnt[kScanItems];
+        const uint32_t b = base + q * kScanItems;
+        const uint32_t bits = scan_load(a, b, cnt);
 #pragma unroll
-    for (int i = 0; i < kScanItems; ++i) {
-        if ((bits >> i) & 1u) {
-            a.surv_gid[r] = base + i;
-            a.surv_start[r] = pt;
-            ++r;
-            pt += cnt[i];
+        for (int i = 0; i < kScanItems; ++i) {
+            if ((bits >> i) & 1u) {
+                a.surv_gid[r] = b + i;
+                a.surv_start[r] = pt;
+                ++r;
+                pt += cnt[i];
+            }
         }
     }
 }
@@ -1282,7 +1295,8 @@ void launch_preprocess_compressed(const PreprocessArgs& a, const SceneCompressed
     preprocess_kernel<SceneCompressed><<<preprocess_grid_size<SceneCompressed>(a.n), 256, 0, stream>>>(a, s);
 }
 
-uint32_t scan_tile_count(uint32_t n) { return (n + kScanTile - 1) / kScanTile; }
+static_assert(kScanTile == kScanTileGaussians, "scan tile size");
+uint32_t scan_tile_count(uint32_t n) { return (uint32_t)(((uint64_t)n + kScanTile - 1) / kScanTile); }
 
 void launch_scan(const ScanArgs& a, uint32_t scan_tiles, cudaStream_t stream) {
     if (scan_tiles == 0) {
@@ -1425,13 +1439,15 @@ void launch_progressive(uint8_t* image, float* cur_color, float* accum, int widt
 // inside a CUDA-graph capture or a stream-ordered pipeline where cudaMalloc would synchronise
 // the device, a host with a fixed device-memory pool or budget enforced by its own allocator,
 // or a plugin host that owns every buffer and forbids its plugins from allocating. For them
-// the scan's only scratch — the survivor and point totals of every 4096-Gaussian tile — lives
+// the scan's only scratch — the survivor and point totals of every 16384-Gaussian tile — lives
 // in this file-scope device array, and the caller passes all inputs and outputs. The array is
 // shared by every call on a device and keeps the previous call's contents; each call rewrites
 // every word it reads before reading it (tile totals, then prefixes); calls that overlap on the GPU
 // (different streams, or host threads on the same device) race on it and must be serialised.
 // ---------------------------------------------------------------------------------
-constexpr uint32_t kNoAllocScanMaxTiles = 65536;  // 512 KiB of tile words: n <= 2^28 Gaussians
+constexpr uint32_t kNoAllocScanMaxTiles = 65536;  // 512 KiB of tile words
+constexpr uint64_t kNoAllocScanMaxGaussians = 1ull << 28;  // the stated limit (16,384 tiles used)
+static_assert(kNoAllocScanMaxGaussians / kScanTile <= kNoAllocScanMaxTiles, "scratch too small");
 static __device__ __align__(256) unsigned long long g_noalloc_scan_scratch[kNoAllocScanMaxTiles + 1];
 
 namespace {
@@ -1447,10 +1463,9 @@ extern "C" gps_status gps_workload_scan_noalloc(const uint32_t* d_counts, const 
                                                 uint32_t* d_tile_first_rank, uint32_t* d_counters8, void* stream) {
     using namespace gps;
     const uint64_t tiles64 = ((uint64_t)n + kScanTile - 1) / kScanTile;
-    if (tiles64 > kNoAllocScanMaxTiles) {
-        set_last_error("gps_workload_scan_noalloc: " + std::to_string(n) + " Gaussians exceed the fixed scratch of " +
-                       std::to_string(kNoAllocScanMaxTiles) + " tiles (" +
-                       std::to_string((unsigned long long)kNoAllocScanMaxTiles * kScanTile) + " Gaussians)");
+    if ((uint64_t)n > kNoAllocScanMaxGaussians) {
+        set_last_error("gps_workload_scan_noalloc: " + std::to_string(n) + " Gaussians exceed the fixed scratch's limit of " +
+                       std::to_string((unsigned long long)kNoAllocScanMaxGaussians) + " Gaussians");
         return GPS_ERR_SIZE;
     }
     const uint32_t tiles = (uint32_t)tiles64;

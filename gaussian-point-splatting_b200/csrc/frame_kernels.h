@@ -133,6 +133,7 @@ void launch_tile_nodes(const float4* src, uint32_t src_pb, uint32_t src_n, uint3
                        const float2* offsets, uint64_t total, float4* dst, uint32_t nodes, cudaStream_t stream);
 void launch_scan(const ScanArgs& a, uint32_t scan_tiles, cudaStream_t stream);
 uint32_t scan_tile_count(uint32_t n);
+constexpr uint32_t kScanTileGaussians = 16384;  // Gaussians per scan tile (counts are padded to it)
 void launch_splat(const SplatArgs& a, int grid, int block, cudaStream_t stream);
 void launch_clear(uint64_t* buf, uint64_t entries, uint64_t value, cudaStream_t stream);
 void launch_resolve(const ResolveArgs& a, bool depth_only, cudaStream_t stream);

@@ -690,7 +690,7 @@ gps_status create_renderer(gps_scene* scene, const gps_settings* settings, const
     r->cap_blocks = std::max<uint32_t>(scene->block_count, cap_blocks);
     r->n = r->cap_n;  // size the per-Gaussian arrays for the capacity, then bind the scene
     r->scan_tiles = scan_tile_count(r->n);
-    r->n_pad = r->scan_tiles * 4096;
+    r->n_pad = r->scan_tiles * kScanTileGaussians;
     r->cap_entries = std::max(entries, cap_entries);
     try {
         r->buffer.reset(dev_alloc<uint64_t>(r->cap_entries));
@@ -736,7 +736,7 @@ gps_status create_renderer(gps_scene* scene, const gps_settings* settings, const
     }
     r->n = (uint32_t)scene->n;
     r->scan_tiles = scan_tile_count(r->n);
-    r->n_pad = r->scan_tiles * 4096;
+    r->n_pad = r->scan_tiles * kScanTileGaussians;
     *out = r.release();
     return GPS_OK;
 }
@@ -748,7 +748,7 @@ gps_status bind_scene(gps_renderer* r, gps_scene* scene) {
     r->scene = scene;
     r->n = (uint32_t)scene->n;
     r->scan_tiles = scan_tile_count(r->n);
-    r->n_pad = r->scan_tiles * 4096;
+    r->n_pad = r->scan_tiles * kScanTileGaussians;
     return GPS_OK;
 }
 
