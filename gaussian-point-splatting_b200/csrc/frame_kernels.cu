@@ -26,8 +26,11 @@ namespace {
 
 constexpr int kScanThreads = 256;
 constexpr int kScanItems = 16;   // per thread and round
-constexpr int kScanRounds = 4;   // a thread covers kScanItems * kScanRounds consecutive Gaussians
-constexpr uint32_t kScanTile = kScanThreads * kScanItems * kScanRounds;  // 16384 Gaussians per scan tile
+constexpr int kScanRoundsMax = 4;  // a thread covers kScanItems * rounds consecutive Gaussians:
+                                   // 1 round (4096-Gaussian tiles) below kScanBigScene, else 4
+constexpr uint32_t kScanTile = kScanThreads * kScanItems * kScanRoundsMax;  // largest tile, 16384
+constexpr uint32_t kScanTileSmall = kScanThreads * kScanItems;             // 4096
+constexpr uint32_t kScanBigScene = 32u << 20;
 
 // ---------------------------------------------------------------------------------
 // Hi-Z query (depth_mip_chain.cuh:172-215, the non-tree variant the reference compiles)
@@ -359,9 +362,10 @@ __device__ __forceinline__ void block_scan_pair(uint32_t s, uint32_t p, uint32_t
 }
 
 // Pass 1 of the scan: every tile's survivor and point totals, fully parallel.
+template <int kScanRounds>
 __global__ void __launch_bounds__(kScanThreads) scan_reduce_kernel(ScanArgs a) {
     const uint32_t tile = blockIdx.x;
-    const uint32_t base = tile * kScanTile + threadIdx.x * (kScanItems * kScanRounds);
+    const uint32_t base = tile * (kScanThreads * kScanItems * kScanRounds) + threadIdx.x * (kScanItems * kScanRounds);
     uint32_t surv = 0, pts = 0;
 #pragma unroll
     for (int q = 0; q < kScanRounds; ++q) {
@@ -425,9 +429,10 @@ __global__ void __launch_bounds__(kTileScanThreads) scan_tiles_kernel(ScanArgs a
 
 // Pass 3: each tile rescans its Gaussians from its prefix and writes the compacted survivor
 // ids and first points.
+template <int kScanRounds>
 __global__ void __launch_bounds__(kScanThreads) scan_write_kernel(ScanArgs a) {
     const uint32_t tile = blockIdx.x;
-    const uint32_t base = tile * kScanTile + threadIdx.x * (kScanItems * kScanRounds);
+    const uint32_t base = tile * (kScanThreads * kScanItems * kScanRounds) + threadIdx.x * (kScanItems * kScanRounds);
     uint32_t surv = 0, pts = 0;
 #pragma unroll
     for (int q = 0; q < kScanRounds; ++q) {
@@ -1296,16 +1301,25 @@ void launch_preprocess_compressed(const PreprocessArgs& a, const SceneCompressed
 }
 
 static_assert(kScanTile == kScanTileGaussians, "scan tile size");
-uint32_t scan_tile_count(uint32_t n) { return (uint32_t)(((uint64_t)n + kScanTile - 1) / kScanTile); }
+// tile words a scan of n Gaussians may use (the small-tile count, an upper bound)
+uint32_t scan_tile_count(uint32_t n) { return (uint32_t)(((uint64_t)n + kScanTileSmall - 1) / kScanTileSmall); }
 
 void launch_scan(const ScanArgs& a, uint32_t scan_tiles, cudaStream_t stream) {
-    if (scan_tiles == 0) {
+    if (scan_tiles == 0 || a.n == 0) {
         cudaMemsetAsync(a.counters, 0, sizeof(PassCounters), stream);
         return;
     }
-    scan_reduce_kernel<<<scan_tiles, kScanThreads, 0, stream>>>(a);
-    scan_tiles_kernel<<<1, kTileScanThreads, 0, stream>>>(a, scan_tiles);
-    scan_write_kernel<<<scan_tiles, kScanThreads, 0, stream>>>(a);
+    if (a.n >= kScanBigScene) {  // fewer, larger tiles: four rounds per thread
+        const uint32_t tiles = (uint32_t)(((uint64_t)a.n + kScanTile - 1) / kScanTile);
+        scan_reduce_kernel<kScanRoundsMax><<<tiles, kScanThreads, 0, stream>>>(a);
+        scan_tiles_kernel<<<1, kTileScanThreads, 0, stream>>>(a, tiles);
+        scan_write_kernel<kScanRoundsMax><<<tiles, kScanThreads, 0, stream>>>(a);
+    } else {
+        const uint32_t tiles = (uint32_t)(((uint64_t)a.n + kScanTileSmall - 1) / kScanTileSmall);
+        scan_reduce_kernel<1><<<tiles, kScanThreads, 0, stream>>>(a);
+        scan_tiles_kernel<<<1, kTileScanThreads, 0, stream>>>(a, tiles);
+        scan_write_kernel<1><<<tiles, kScanThreads, 0, stream>>>(a);
+    }
     const uint64_t max_tiles = ((uint64_t)a.max_points + a.tile_points - 1) / a.tile_points;
     const uint64_t want = (max_tiles + 255) / 256;
     const int owner_grid = (int)(want < 1184 ? (want ? want : 1) : 1184);  // 148 SMs x 8
@@ -1439,15 +1453,15 @@ void launch_progressive(uint8_t* image, float* cur_color, float* accum, int widt
 // inside a CUDA-graph capture or a stream-ordered pipeline where cudaMalloc would synchronise
 // the device, a host with a fixed device-memory pool or budget enforced by its own allocator,
 // or a plugin host that owns every buffer and forbids its plugins from allocating. For them
-// the scan's only scratch — the survivor and point totals of every 16384-Gaussian tile — lives
+// the scan's only scratch — the survivor and point totals of every scan tile — lives
 // in this file-scope device array, and the caller passes all inputs and outputs. The array is
 // shared by every call on a device and keeps the previous call's contents; each call rewrites
 // every word it reads before reading it (tile totals, then prefixes); calls that overlap on the GPU
 // (different streams, or host threads on the same device) race on it and must be serialised.
 // ---------------------------------------------------------------------------------
 constexpr uint32_t kNoAllocScanMaxTiles = 65536;  // 512 KiB of tile words
-constexpr uint64_t kNoAllocScanMaxGaussians = 1ull << 28;  // the stated limit (16,384 tiles used)
-static_assert(kNoAllocScanMaxGaussians / kScanTile <= kNoAllocScanMaxTiles, "scratch too small");
+constexpr uint64_t kNoAllocScanMaxGaussians = 1ull << 28;  // the stated limit
+static_assert(kNoAllocScanMaxGaussians / kScanTileSmall <= kNoAllocScanMaxTiles, "scratch too small");
 static __device__ __align__(256) unsigned long long g_noalloc_scan_scratch[kNoAllocScanMaxTiles + 1];
 
 namespace {
