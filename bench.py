@@ -189,6 +189,35 @@ def barrier(world: int):
 # ---------------------------------------------------------------------------------
 # CPU baseline (the oracle, oracle/oracle.cpp) on a bounded sample of the workload
 # ---------------------------------------------------------------------------------
+def stage_rooflines(stages, spec, n, entries, surv, passes, w, h, peak):
+    """Achieved algorithmic GB/s of the HBM-bound stages, per launch, against the measured copy
+    peak.  Algorithmic bytes per launch (survivors from the device counters, FP32 scene):
+      preprocess  n/8 mask (+ n/8 previous mask in pass 2) + 48 per tested Gaussian
+                  (position, rotation, scale; an upper bound: culled chunks are skipped)
+                  + per survivor 192 SH + 64 record + 4 count
+      scan        n/8 mask, read twice, + 4 per survivor count read twice + 8 per survivor written
+      resolve     8 per splat-buffer entry + 16 per pixel (final) / 4 (depth-only), averaged
+      clear       8 per splat-buffer entry"""
+    out = {}
+    s_pass = surv / max(1, passes)
+    model = {
+        "preprocess": (n / 8.0 + n * 48.0 + s_pass * (192.0 + 64.0 + 4.0)) if spec.get("fmt") != "half" else None,
+        "scan": n / 4.0 + s_pass * (8.0 + 8.0),
+        "resolve": 8.0 * entries + (10.0 if passes == 2 else 16.0) * w * h,
+        "clear": 8.0 * entries,
+    }
+    for k, b in model.items():
+        ms, launches = stages.get(k, (0.0, 0))
+        if b is None or ms <= 0 or launches <= 0:
+            continue
+        if k == "scan":
+            launches = max(1, launches // 4)  # four launches per pass scan
+        per = ms / launches
+        gbs = b / (per / 1000.0) / 1e9
+        out[k] = {"achieved_gbs": gbs, "frac": gbs / peak, "ms_per_launch": per, "algorithmic_bytes": b}
+    return out
+
+
 def measured_traffic(kernel: str, spec):
     """DRAM bytes per splat launch from the committed ncu summary (dram__bytes_read.sum +
     dram__bytes_write.sum, averaged over a frame's two launches).  The splat's traffic follows
@@ -631,6 +660,7 @@ def main():
         "gpu_launches": int(launches_per_frame * K),
         "roofline": roofline,
         "stages_ms_per_frame": {k: v[0] / K for k, v in stages.items()},
+        "stage_rooflines": stage_rooflines(stages, spec, n_scene, entries, surv, passes, w, h, hbm_peak),
         "points_per_frame": [st.num_points_one, st.num_points_two],
         "survivors_per_frame": [st.survivors_one, st.survivors_two],
     }
