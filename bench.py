@@ -192,16 +192,18 @@ def barrier(world: int):
 def stage_rooflines(stages, spec, n, entries, surv, passes, w, h, peak):
     """Achieved algorithmic GB/s of the HBM-bound stages, per launch, against the measured copy
     peak.  Algorithmic bytes per launch (survivors from the device counters, FP32 scene):
-      preprocess  n/8 mask (+ n/8 previous mask in pass 2) + 48 per tested Gaussian
-                  (position, rotation, scale; an upper bound: culled chunks are skipped)
-                  + per survivor 192 SH + 64 record + 4 count
+      preprocess  n/8 mask + 48 per Gaussian (position, rotation, scale) + per survivor 192 SH
+                  + 64 record + 4 count; reported without block culling only (every Gaussian
+                  is then tested)
       scan        n/8 mask, read twice, + 4 per survivor count read twice + 8 per survivor written
       resolve     8 per splat-buffer entry + 16 per pixel (final) / 4 (depth-only), averaged
       clear       8 per splat-buffer entry"""
     out = {}
     s_pass = surv / max(1, passes)
     model = {
-        "preprocess": (n / 8.0 + n * 48.0 + s_pass * (192.0 + 64.0 + 4.0)) if spec.get("fmt") != "half" else None,
+        # without block culling every Gaussian is tested; with it the tested count is unknown here
+        "preprocess": (n / 8.0 + n * 48.0 + s_pass * (192.0 + 64.0 + 4.0))
+        if spec.get("fmt") != "half" and not spec.get("hier") else None,
         "scan": n / 4.0 + s_pass * (8.0 + 8.0),
         "resolve": 8.0 * entries + (10.0 if passes == 2 else 16.0) * w * h,
         "clear": 8.0 * entries,
