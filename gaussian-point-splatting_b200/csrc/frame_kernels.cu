@@ -563,6 +563,9 @@ __device__ __forceinline__ void splat_point_biased(uint32_t point, const SplatRe
 #ifndef GPS_SPLAT_PRETEST
 #define GPS_SPLAT_PRETEST 1
 #endif
+#ifndef GPS_SPLAT_PIPELINE
+#define GPS_SPLAT_PIPELINE 1
+#endif
 constexpr int kSplatBatch = GPS_SPLAT_BATCH;
 
 __device__ __forceinline__ void splat_point_unbiased(uint32_t point, const SplatRecord& rec, const FrameConst& fc,
@@ -692,6 +695,35 @@ __device__ __forceinline__ void splat_point_unbiased_k(uint32_t point, const Spl
     c.tiles_per_row = (fc.up_width + kTileSize - 1) >> kTileBits;
     const unsigned long long key = (unsigned long long)rec.d.z | ((unsigned long long)rec.d.w << 32);
     unsigned long long* buf = reinterpret_cast<unsigned long long*>(buffer);
+#if GPS_SPLAT_PRETEST && GPS_SPLAT_PIPELINE
+    // Software-pipelined over passes: pass p+1's samples are drawn and their pre-test loads
+    // issued before pass p's atomics consume its loads, so the load latency hides behind the
+    // next pass's arithmetic.  Samples are still drawn in stream order.
+    uint32_t sa[K], sb[K];
+    bool la[K], lb[K];
+    unsigned long long va[K], vb[K];
+    auto draw = [&](int p, uint32_t* sl, bool* lv, unsigned long long* vv) {
+#pragma unroll
+        for (int j = 0; j < K; ++j) lv[j] = draw_sample(seed, c, p, sl[j]);
+#pragma unroll
+        for (int j = 0; j < K; ++j)
+            vv[j] = lv[j] ? (GPS_SPLAT_PRETEST == 1 ? __ldca(buf + sl[j]) : __ldcg(buf + sl[j])) : 0ull;
+    };
+    auto commit = [&](const uint32_t* sl, const bool* lv, const unsigned long long* vv) {
+#pragma unroll
+        for (int j = 0; j < K; ++j)
+            if (lv[j] && vv[j] > key) atomicMin(buf + sl[j], key);
+    };
+    if (c.passes > 0) draw(0, sa, la, va);
+    for (int p = 0; p < c.passes; p += 2) {
+        if (p + 1 < c.passes) draw(p + 1, sb, lb, vb);
+        commit(sa, la, va);
+        if (p + 1 < c.passes) {
+            if (p + 2 < c.passes) draw(p + 2, sa, la, va);
+            commit(sb, lb, vb);
+        }
+    }
+#else
     for (int p = 0; p < c.passes; ++p) {
         uint32_t slot[K];
         bool live[K];
@@ -706,6 +738,7 @@ __device__ __forceinline__ void splat_point_unbiased_k(uint32_t point, const Spl
 #endif
         }
     }
+#endif
 }
 
 // K > 0: unbiased splatting with K points per thread per pass; K = 0: any other setting.
