@@ -886,6 +886,9 @@ __global__ void __launch_bounds__(256) resolve_morton_kernel(ResolveArgs a, int 
 // word after each pixel's samples keeps the threads of a warp, which read samples a whole
 // pixel run apart, on different banks.  Used when SS*SS*spp is a power of two >= 2.
 constexpr int kResolveStageBytes = 48 * 1024;
+#ifndef GPS_RESOLVE_PIXELS
+#define GPS_RESOLVE_PIXELS 128
+#endif
 
 template <bool kDepthOnly>
 __global__ void __launch_bounds__(256) resolve_staged_kernel(ResolveArgs a, int ss_log2, int run_log2) {
@@ -1414,7 +1417,7 @@ void launch_resolve(const ResolveArgs& a, bool depth_only, cudaStream_t stream) 
         for (int l = 1; l <= 12; ++l)
             if (run == (1u << l)) run_log2 = l;
         const uint32_t run_bytes = (run + 1u) * 8u;                 // with the pad word
-        uint32_t px = 256;
+        uint32_t px = GPS_RESOLVE_PIXELS;  // pixels (threads) per block
         while (px > 32 && px * run_bytes > (uint32_t)kResolveStageBytes) px >>= 1;
         if (run_log2 > 0 && px * run_bytes <= (uint32_t)kResolveStageBytes && (uint64_t)a.entries <= 0x7FFFFFFFull) {
             const unsigned grid = (unsigned)((threads + px - 1) / px);
