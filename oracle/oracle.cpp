@@ -34,28 +34,39 @@
 
 #include "../include/gps_b200.h"
 
+// The estimator's arithmetic type: float for the FP32 oracle (the checker of the CUDA path),
+// double for the FP64 build (ORACLE_FP64, liboracle64.so) used to state arithmetic error.  The
+// integer layer (seeds, PCG, Morton addressing, packing, scan) is the same in both; scene storage,
+// the depth chain and the culling blocks stay FP32 in both.
+#ifdef ORACLE_FP64
+typedef double real;
+#else
+typedef float real;
+#endif
+
+
 namespace {
 
 // ---------------------------------------------------------------------------------
 // small math (column-major), same association as the reference
 // ---------------------------------------------------------------------------------
-struct V2 { float x, y; };
-struct V3 { float x, y, z; };
-struct V4 { float x, y, z, w; };
+struct V2 { real x, y; };
+struct V3 { real x, y, z; };
+struct V4 { real x, y, z, w; };
 struct M3 { V3 c[3]; };
 struct M4 { V4 c[4]; };
 
-inline float gmin(float x, float y) { return (y < x) ? y : x; }
-inline float gmax(float x, float y) { return (x < y) ? y : x; }
-inline float gclamp(float x, float lo, float hi) { return gmin(gmax(x, lo), hi); }
-inline V3 v3(float x, float y, float z) { return {x, y, z}; }
-inline V4 v4(float x, float y, float z, float w) { return {x, y, z, w}; }
+inline real gmin(real x, real y) { return (y < x) ? y : x; }
+inline real gmax(real x, real y) { return (x < y) ? y : x; }
+inline real gclamp(real x, real lo, real hi) { return gmin(gmax(x, lo), hi); }
+inline V3 v3(real x, real y, real z) { return {x, y, z}; }
+inline V4 v4(real x, real y, real z, real w) { return {x, y, z, w}; }
 inline V3 add(V3 a, V3 b) { return {a.x + b.x, a.y + b.y, a.z + b.z}; }
 inline V3 sub(V3 a, V3 b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
-inline V3 mul(V3 a, float s) { return {a.x * s, a.y * s, a.z * s}; }
+inline V3 mul(V3 a, real s) { return {a.x * s, a.y * s, a.z * s}; }
 inline V4 add(V4 a, V4 b) { return {a.x + b.x, a.y + b.y, a.z + b.z, a.w + b.w}; }
-inline V4 mul(V4 a, float s) { return {a.x * s, a.y * s, a.z * s, a.w * s}; }
-inline float dot3(V3 a, V3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+inline V4 mul(V4 a, real s) { return {a.x * s, a.y * s, a.z * s, a.w * s}; }
+inline real dot3(V3 a, V3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
 inline M3 mat3_of(const M4& m) {
     return {{{m.c[0].x, m.c[0].y, m.c[0].z}, {m.c[1].x, m.c[1].y, m.c[1].z}, {m.c[2].x, m.c[2].y, m.c[2].z}}};
 }
@@ -82,14 +93,14 @@ M4 m4_from(const float* p) {
     for (int c = 0; c < 4; ++c) m.c[c] = v4(p[4 * c], p[4 * c + 1], p[4 * c + 2], p[4 * c + 3]);
     return m;
 }
-inline float el(const M4& m, int c, int r) { const V4& v = m.c[c]; return r == 0 ? v.x : r == 1 ? v.y : r == 2 ? v.z : v.w; }
-inline float el3(const M3& m, int c, int r) { const V3& v = m.c[c]; return r == 0 ? v.x : r == 1 ? v.y : v.z; }
+inline real el(const M4& m, int c, int r) { const V4& v = m.c[c]; return r == 0 ? v.x : r == 1 ? v.y : r == 2 ? v.z : v.w; }
+inline real el3(const M3& m, int c, int r) { const V3& v = m.c[c]; return r == 0 ? v.x : r == 1 ? v.y : v.z; }
 
 M3 inverse3(const M3& m) {
     auto e = [&](int c, int r) { return el3(m, c, r); };
-    float od = 1.0f / (+e(0, 0) * (e(1, 1) * e(2, 2) - e(2, 1) * e(1, 2)) - e(1, 0) * (e(0, 1) * e(2, 2) - e(2, 1) * e(0, 2)) +
+    real od = 1.0f / (+e(0, 0) * (e(1, 1) * e(2, 2) - e(2, 1) * e(1, 2)) - e(1, 0) * (e(0, 1) * e(2, 2) - e(2, 1) * e(0, 2)) +
                        e(2, 0) * (e(0, 1) * e(1, 2) - e(1, 1) * e(0, 2)));
-    float i[3][3];
+    real i[3][3];
     i[0][0] = +(e(1, 1) * e(2, 2) - e(2, 1) * e(1, 2));
     i[1][0] = -(e(1, 0) * e(2, 2) - e(2, 0) * e(1, 2));
     i[2][0] = +(e(1, 0) * e(2, 1) - e(2, 0) * e(1, 1));
@@ -148,16 +159,16 @@ inline Seed pcg_step(Seed s) {
 }
 inline V2 pcg2d(Seed& s) {
     s = pcg_step(s);
-    return {(float)s.x * 2.3283064365387e-10f, (float)s.y * 2.3283064365387e-10f};
+    return {(real)s.x * 2.3283064365387e-10f, (real)s.y * 2.3283064365387e-10f};
 }
-inline int stochastic_round(float x, float u) {
+inline int stochastic_round(real x, real u) {
     int base = (int)std::floor(x);
-    float frac = x - (float)base;
+    real frac = x - (real)base;
     int r = (u < frac) ? base + 1 : base;
     return r < 0 ? 0 : r;
 }
-float dilog(float x) {
-    float y = -6.09201442e-01f;
+real dilog(real x) {
+    real y = -6.09201442e-01f;
     y = std::fmaf(y, x, 1.79126616e+00f);
     y = std::fmaf(y, x, -2.14953223e+00f);
     y = std::fmaf(y, x, 1.26304372e+00f);
@@ -165,13 +176,13 @@ float dilog(float x) {
     y = std::fmaf(y, x, -1.87417414e-01f);
     y = std::fmaf(y, x, 1.99603130e+00f);
     y = std::fmaf(y, x, 5.99669467e-05f);
-    float s = 1.0f - x;
+    real s = 1.0f - x;
     if (s > 0.0f) y += s * std::log(std::fmax(s, 1e-37f));
     return y;
 }
-float inv_dilog(float x) {
-    float t = std::fmin(x / 1.6449340668482264f, 1.0f);
-    float y = -1.27463503e+01f;
+real inv_dilog(real x) {
+    real t = std::fmin(x / 1.6449340668482264f, 1.0f);
+    real y = -1.27463503e+01f;
     y = std::fmaf(y, t, 5.88993459e+01f);
     y = std::fmaf(y, t, -1.16025780e+02f);
     y = std::fmaf(y, t, 1.26945827e+02f);
@@ -184,26 +195,26 @@ float inv_dilog(float x) {
     y = std::fmaf(y, t, -2.82836687e-05f);
     return y;
 }
-constexpr float kTwoPiF = 2.0f * 3.141592654f;
-V2 box_muller(float u1, float u2) {
-    float r = std::sqrt(std::fmax(-2.0f * std::log(gclamp(u1, 1.e-37f, 1.0f)), 0.0f));
-    float th = kTwoPiF * u2;
+constexpr real kTwoPiF = 2.0f * 3.141592654f;
+V2 box_muller(real u1, real u2) {
+    real r = std::sqrt(std::fmax(-2.0f * std::log(gclamp(u1, 1.e-37f, 1.0f)), 0.0f));
+    real th = kTwoPiF * u2;
     return {r * std::cos(th), r * std::sin(th)};
 }
-V2 corrected_box_muller(float u1, float u2, float alpha) {
-    float a = 1.0f / std::fmax(alpha, 1.e-37f) * inv_dilog((1.0f - u1) * dilog(alpha));
+V2 corrected_box_muller(real u1, real u2, real alpha) {
+    real a = 1.0f / std::fmax(alpha, 1.e-37f) * inv_dilog((1.0f - u1) * dilog(alpha));
     a = gclamp(a, 1.e-37f, 1.0f);
-    float r = std::sqrt(std::fmax(-2.0f * std::log(a), 0.0f));
-    float th = kTwoPiF * u2;
+    real r = std::sqrt(std::fmax(-2.0f * std::log(a), 0.0f));
+    real th = kTwoPiF * u2;
     return {r * std::cos(th), r * std::sin(th)};
 }
-uint32_t poisson(Seed& st, float lambda) {
+uint32_t poisson(Seed& st, real lambda) {
     V2 u = pcg2d(st);
-    float w = box_muller(u.x, u.y).x;
-    float w2 = w * w, w3 = w2 * w, w4 = w2 * w2;
-    float s = std::sqrt(lambda);
-    float inv_s = 1.0f / s, inv_l = 1.0f / lambda;
-    float kf = lambda + s * w + (w2 - 1.0f) / 6.0f;
+    real w = box_muller(u.x, u.y).x;
+    real w2 = w * w, w3 = w2 * w, w4 = w2 * w2;
+    real s = std::sqrt(lambda);
+    real inv_s = 1.0f / s, inv_l = 1.0f / lambda;
+    real kf = lambda + s * w + (w2 - 1.0f) / 6.0f;
     kf += inv_s * (-(1.0f / 36.0f) * w - (1.0f / 72.0f) * w3);
     kf += inv_l * (-(8.0f / 405.0f) + (7.0f / 810.0f) * w2 + (1.0f / 270.0f) * w4);
     long ki = std::lrint(kf);  // round half to even like __float2int_rn
@@ -214,8 +225,8 @@ uint32_t poisson(Seed& st, float lambda) {
 // geometry
 // ---------------------------------------------------------------------------------
 M3 quat_to_rotmat(V4 q) {
-    const float w = q.x, x = q.y, y = q.z, z = q.w;
-    float qxx = x * x, qyy = y * y, qzz = z * z, qxz = x * z, qxy = x * y, qyz = y * z, qwx = w * x, qwy = w * y, qwz = w * z;
+    const real w = q.x, x = q.y, y = q.z, z = q.w;
+    real qxx = x * x, qyy = y * y, qzz = z * z, qxz = x * z, qxy = x * y, qyz = y * z, qwx = w * x, qwy = w * y, qwz = w * z;
     M3 r;
     r.c[0] = v3(1.0f - 2.0f * (qyy + qzz), 2.0f * (qxy + qwz), 2.0f * (qxz - qwy));
     r.c[1] = v3(2.0f * (qxy - qwz), 1.0f - 2.0f * (qxx + qzz), 2.0f * (qyz + qwx));
@@ -232,8 +243,8 @@ V3 transform_point4x3(V3 p, const M4& m) { return add(mul(mat3_of(m), p), v3(m.c
 V3 compute_cov2d(const M4& view, const M3& cov3d, V3 mean, V2 tan_fov, V2 focal) {
     M3 w = mat3_of(view);
     V3 t = transform_point4x3(mean, view);
-    float limx = 1.3f * tan_fov.x, limy = 1.3f * tan_fov.y;
-    float txtz = t.x / t.z, tytz = t.y / t.z;
+    real limx = 1.3f * tan_fov.x, limy = 1.3f * tan_fov.y;
+    real txtz = t.x / t.z, tytz = t.y / t.z;
     t.x = std::fmin(limx, std::fmax(-limx, txtz)) * t.z;
     t.y = std::fmin(limy, std::fmax(-limy, tytz)) * t.z;
     M3 j = {{{focal.x / t.z, 0.0f, -(focal.x * t.x) / (t.z * t.z)}, {0.0f, focal.y / t.z, -(focal.y * t.y) / (t.z * t.z)}, {0.0f, 0.0f, 0.0f}}};
@@ -244,7 +255,7 @@ V3 compute_cov2d(const M4& view, const M3& cov3d, V3 mean, V2 tan_fov, V2 focal)
 bool tile_bounds(int& mnx, int& mny, int& mxx, int& mxy, int resx, int resy, V3 cov2d, V2 pm) {
     const int tile = 16;
     int ex = (int)std::ceil(3.0f * std::sqrt(cov2d.x)), ey = (int)std::ceil(3.0f * std::sqrt(cov2d.z));
-    float lox = pm.x - (float)ex, loy = pm.y - (float)ey, hix = pm.x + (float)ex, hiy = pm.y + (float)ey;
+    real lox = pm.x - (real)ex, loy = pm.y - (real)ey, hix = pm.x + (real)ex, hiy = pm.y + (real)ey;
     int tmnx = (int)std::floor(lox / tile), tmny = (int)std::floor(loy / tile);
     int tmxx = (int)std::ceil(hix / tile), tmxy = (int)std::ceil(hiy / tile);
     int tx = (resx + tile - 1) / tile, ty = (resy + tile - 1) / tile;
@@ -259,13 +270,13 @@ bool tile_bounds(int& mnx, int& mny, int& mxx, int& mxy, int resx, int resy, V3 
     mxy = tmxy * tile;
     return true;
 }
-inline uint64_t depth_key(float d, float n, float f) {
-    float t = gclamp((std::fabs(d) - n) / (f - n), 0.0f, 1.0f);
+inline uint64_t depth_key(real d, real n, real f) {
+    real t = gclamp((std::fabs(d) - n) / (f - n), 0.0f, 1.0f);
     return ((uint64_t)(t * 268435456.0f)) & 0xFFFFFFFull;
 }
-inline float view_depth_from_key(uint64_t d, float n, float f) { return -(((float)d / 268435456.0f) * (f - n) + n); }
-inline float view_to_ndc(float z, float n, float f) {
-    float a = (f + n) / (f - n), b = (2.0f * f * n) / (f - n);
+inline real view_depth_from_key(uint64_t d, real n, real f) { return -(((real)d / 268435456.0f) * (f - n) + n); }
+inline real view_to_ndc(real z, real n, real f) {
+    real a = (f + n) / (f - n), b = (2.0f * f * n) / (f - n);
     return a + b / z;
 }
 inline uint32_t spread(uint32_t a) {
@@ -290,11 +301,11 @@ V3 normalize3(V3 v) { return mul(v, 1.0f / std::sqrt(dot3(v, v))); }
 V3 sh_color_fp32(V3 pos, V3 campos, const float* sh) {
     V3 dir = normalize3(sub(pos, campos));
     auto S = [&](int i) { return v3(sh[3 * i], sh[3 * i + 1], sh[3 * i + 2]); };
-    const float C0 = 0.28209479177387814f, C1 = 0.4886025119029199f;
+    const real C0 = 0.28209479177387814f, C1 = 0.4886025119029199f;
     V3 r = mul(S(0), C0);
-    float x = dir.x, y = dir.y, z = dir.z;
+    real x = dir.x, y = dir.y, z = dir.z;
     r = sub(add(sub(r, mul(S(1), C1 * y)), mul(S(2), C1 * z)), mul(S(3), C1 * x));
-    float xx = x * x, yy = y * y, zz = z * z, xy = x * y, yz = y * z, xz = x * z;
+    real xx = x * x, yy = y * y, zz = z * z, xy = x * y, yz = y * z, xz = x * z;
     V3 b2 = add(add(add(add(mul(S(4), 1.0925484305920792f * xy), mul(S(5), -1.0925484305920792f * yz)),
                         mul(S(6), 0.31539156525252005f * (2.0f * zz - xx - yy))),
                     mul(S(7), -1.0925484305920792f * xz)),
@@ -315,7 +326,7 @@ V3 sh_color_fp32(V3 pos, V3 campos, const float* sh) {
 // ---------------------------------------------------------------------------------
 // the oracle context: one scene + settings + frame state
 // ---------------------------------------------------------------------------------
-struct Gaussian {
+struct Gaussian {  // the caller's CPUGaussian layout, kept in FP32
     float mean[3];
     float sh[48];
     float opacity;
@@ -327,14 +338,14 @@ struct Hiz {
     int w = 0, h = 0, levels = 0;
     std::vector<int> lw, lh;
     std::vector<size_t> off;
-    std::vector<float> mip;
+    std::vector<float> mip;  // depth chain, FP32 like the caller's depth image
 };
 
 struct Record {
-    float pm[2], c0, c1, c2, conic[3], opacity;
+    real pm[2], c0, c1, c2, conic[3], opacity;
     int mnx, mny, mxx, mxy;
     uint64_t key;
-    float color[3];
+    real color[3];
 };
 
 struct Ctx {
@@ -345,7 +356,7 @@ struct Ctx {
     std::vector<uint64_t> buffer;
     std::vector<uint32_t> counts, mask[2], block_culled;
     std::vector<Record> rec;
-    std::vector<float> nodes;  // 6 per node (min xyz, max xyz)
+    std::vector<float> nodes;  // 6 per node (min xyz, max xyz), FP32 like the reference's blocks
     uint32_t per_block = 4, node_count = 0;
     uint32_t iteration = 0;
     Hiz hiz;
@@ -414,13 +425,13 @@ void hiz_build(Hiz& h, const float* depth, int min_levels) {
     }
 }
 
-bool hiz_occluded(const Hiz& c, float depth, int mnx, int mny, int mxx, int mxy) {
+bool hiz_occluded(const Hiz& c, real depth, int mnx, int mny, int mxx, int mxy) {
     mnx = std::max(0, mnx);
     mny = std::max(0, mny);
     mxx = std::min(c.w - 1, mxx);
     mxy = std::min(c.h - 1, mxy);
     int d = std::max(mxx - mnx + 1, mxy - mny + 1);
-    int lod = (int)std::ceil(std::log2((float)d / 2.0f));
+    int lod = (int)std::ceil(std::log2((real)d / 2.0f));
     lod = std::min(std::max(lod, 0), c.levels - 1);
     int l = (c.levels - 1) - lod;
     int wl = c.lw[l], hl = c.lh[l];
@@ -445,12 +456,12 @@ FrameC derive(const Ctx& c, const gps_camera* cam) {
     M4 proj = m4_from(cam->proj);
     f.cam = affine_inverse(f.view);
     f.vp = mul(proj, f.view);
-    float r = (float)c.s.width / (float)c.s.height;
-    float tfy = std::tan(c.s.fovy * 0.01745329251994329576923690768489f * 0.5f);
-    float fovx = 2.0f * std::atan(tfy * r);
-    float tfx = std::tan(fovx * 0.5f);
+    real r = (real)c.s.width / (real)c.s.height;
+    real tfy = std::tan(c.s.fovy * 0.01745329251994329576923690768489f * 0.5f);
+    real fovx = 2.0f * std::atan(tfy * r);
+    real tfx = std::tan(fovx * 0.5f);
     f.tan_fov = {tfx, tfy};
-    f.focal = {(float)(c.s.width * c.s.supersampling_factor) / (2.0f * tfx), (float)(c.s.height * c.s.supersampling_factor) / (2.0f * tfy)};
+    f.focal = {(real)(c.s.width * c.s.supersampling_factor) / (2.0f * tfx), (real)(c.s.height * c.s.supersampling_factor) / (2.0f * tfy)};
     for (int i = 0; i < 6; ++i)
         f.planes[i] = v4(cam->frustum_planes[4 * i], cam->frustum_planes[4 * i + 1], cam->frustum_planes[4 * i + 2], cam->frustum_planes[4 * i + 3]);
     return f;
@@ -470,14 +481,14 @@ void block_cull(Ctx& c, const FrameC& f) {
         }
         if (!culled && c.s.enable_occlusion_culling) {
             int minx = c.hiz.w - 1, miny = c.hiz.h - 1, maxx = 0, maxy = 0;
-            float md = 1e30f;
+            real md = 1e30f;
             bool any = false;
             for (int k = 0; k < 8; ++k) {
                 V4 p = v4((k & 1) ? mx.x : mn.x, (k & 2) ? mx.y : mn.y, (k & 4) ? mx.z : mn.z, 1.0f);
                 V4 cl = mul(f.vp, p);
                 if (cl.w <= 0.0f) continue;
                 any = true;
-                float nx = cl.x / cl.w, ny = cl.y / cl.w, nz = cl.z / cl.w;
+                real nx = cl.x / cl.w, ny = cl.y / cl.w, nz = cl.z / cl.w;
                 int px = (int)((nx * 0.5f + 0.5f) * c.hiz.w), py = (int)((ny * 0.5f + 0.5f) * c.hiz.h);
                 minx = std::min(minx, px);
                 miny = std::min(miny, py);
@@ -499,24 +510,24 @@ void block_cull(Ctx& c, const FrameC& f) {
 
 // Geometry of Gaussian idx (loadAndTransformGaussian + the splat's per-Gaussian prologue):
 // fills everything of the record except the colour; false if the Gaussian is rejected.
-bool geometry_record(const Ctx& c, const FrameC& f, uint32_t idx, Record& r, float& ndc_z, float& det_out,
+bool geometry_record(const Ctx& c, const FrameC& f, uint32_t idx, Record& r, real& ndc_z, real& det_out,
                      V3& cov2d_out) {
     const gps_settings& s = c.s;
     const Gaussian& g = c.g[idx];
     V3 mean = v3(g.mean[0], g.mean[1], g.mean[2]);
     V3 view_mean = transform_point4x3(mean, f.view);
-    float view_z = view_mean.z;
+    real view_z = view_mean.z;
     if (-view_z <= 0.2f) return false;
     V4 pmn = mul(f.vp, v4(mean.x, mean.y, mean.z, 1.0f));
     pmn = mul(pmn, 1.0f / pmn.w);
     if (pmn.z < -1.0f || pmn.z > 1.0f) return false;
     M3 cov = scale_rot_to_cov(v3(g.scale[0], g.scale[1], g.scale[2]), v4(g.rot[0], g.rot[1], g.rot[2], g.rot[3]));
     V3 cov2d = compute_cov2d(f.view, cov, mean, f.tan_fov, f.focal);
-    float dil = 0.3f * (float)s.supersampling_factor * (float)s.supersampling_factor;
+    real dil = 0.3f * (real)s.supersampling_factor * (real)s.supersampling_factor;
     cov2d = v3(cov2d.x + dil, cov2d.y + 0.0f, cov2d.z + dil);
-    float det = cov2d.x * cov2d.z - cov2d.y * cov2d.y;
+    real det = cov2d.x * cov2d.z - cov2d.y * cov2d.y;
     if (det <= 0.0f) return false;
-    V2 pm = {(pmn.x * 0.5f + 0.5f) * (float)c.up_w, (pmn.y * 0.5f + 0.5f) * (float)c.up_h};
+    V2 pm = {(pmn.x * 0.5f + 0.5f) * (real)c.up_w, (pmn.y * 0.5f + 0.5f) * (real)c.up_h};
     int mnx, mny, mxx, mxy;
     if (!tile_bounds(mnx, mny, mxx, mxy, c.up_w, c.up_h, cov2d, pm)) return false;
     r.pm[0] = pm.x;
@@ -524,7 +535,7 @@ bool geometry_record(const Ctx& c, const FrameC& f, uint32_t idx, Record& r, flo
     r.c0 = std::sqrt(cov2d.x);
     r.c1 = cov2d.y / r.c0;
     r.c2 = std::sqrt(cov2d.z - r.c1 * r.c1);
-    float inv_det = 1.0f / det;
+    real inv_det = 1.0f / det;
     r.conic[0] = cov2d.z * inv_det;
     r.conic[1] = -cov2d.y * inv_det;
     r.conic[2] = cov2d.x * inv_det;
@@ -561,27 +572,27 @@ uint32_t preprocess_one(const Ctx& c, const FrameC& f, uint32_t idx, int frame_s
         if ((c.block_culled[node >> 5] >> (node & 31)) & 1u) return 0;
     }
     if (only_prev && ((mask_prev[idx >> 5] >> (idx & 31)) & 1u)) return 0;
-    float opacity = gmin(c.g[idx].opacity, 1.0f);
+    real opacity = gmin(c.g[idx].opacity, 1.0f);
     if (opacity <= 0.0f) return 0;
-    float ndc_z, det;
+    real ndc_z, det;
     V3 cov2d;
     if (!geometry_record(c, f, idx, r, ndc_z, det, cov2d)) return 0;
     if (r.mnx >= c.up_w || r.mny >= c.up_h || r.mxx < 0 || r.mxy < 0) return 0;
     if (s.cull_small_gaussians) {
-        float half = 0.5f * (cov2d.x + cov2d.z);
-        float t2 = std::sqrt(std::fmax(0.1f, half * half - det));
+        real half = 0.5f * (cov2d.x + cov2d.z);
+        real t2 = std::sqrt(std::fmax(0.1f, half * half - det));
         if (half + t2 < 0.02f || half - t2 < 0.02f) return 0;
     }
-    float sdet = std::sqrt(det);
-    const float two_pi = 2.0f * 3.14159265358979323846f;
-    float importance = s.use_unbiased_2d_splatting ? two_pi * sdet * dilog(opacity) : opacity * two_pi * sdet;
+    real sdet = std::sqrt(det);
+    const real two_pi = 2.0f * 3.14159265358979323846f;
+    real importance = s.use_unbiased_2d_splatting ? two_pi * sdet * dilog(opacity) : opacity * two_pi * sdet;
     const int ss = s.supersampling_factor;
     if (s.enable_occlusion_culling && hiz_occluded(c.hiz, ndc_z, r.mnx / ss, r.mny / ss, r.mxx / ss, r.mxy / ss))
         return 0;
-    float k = (float)(ss * ss);
+    real k = (real)(ss * ss);
     if (!s.reduce_point_count) k = 1.0f;
     uint32_t n = s.use_unbiased_2d_splatting ? poisson(seed, importance) : (uint32_t)stochastic_round(importance, pcg2d(seed).x);
-    if (k > 1) n = (uint32_t)stochastic_round((float)n / k, pcg2d(seed).x);
+    if (k > 1) n = (uint32_t)stochastic_round((real)n / k, pcg2d(seed).x);
     if (n == 0) return 0;
     uint32_t cap = (uint32_t)(c.up_w * c.up_h / (2 * k));
     n = std::min(n, cap);
@@ -655,12 +666,12 @@ void splat_point(Ctx& c, uint32_t p, const Record& r, int frame_seed) {
     for (int q = 0; q < np * k; ++q) {
         V2 u = pcg2d(seed);
         V2 xy = s.use_unbiased_2d_splatting ? corrected_box_muller(u.x, u.y, r.opacity) : box_muller(u.x, u.y);
-        float px = std::floor(r.pm[0] + r.c0 * xy.x), py = std::floor(r.pm[1] + r.c1 * xy.x + r.c2 * xy.y);
+        real px = std::floor(r.pm[0] + r.c0 * xy.x), py = std::floor(r.pm[1] + r.c1 * xy.x + r.c2 * xy.y);
         int x = (int)px, y = (int)py;
-        float dx = r.pm[0] - px, dy = r.pm[1] - py;
+        real dx = r.pm[0] - px, dy = r.pm[1] - py;
         if (x < r.mnx || x >= r.mxx || y < r.mny || y >= r.mxy) continue;
-        float sig = -0.5f * (r.conic[0] * dx * dx + r.conic[2] * dy * dy) - r.conic[1] * dx * dy;
-        float gw = sig > 0.0f ? 0.0f : std::exp(sig);
+        real sig = -0.5f * (r.conic[0] * dx * dx + r.conic[2] * dy * dy) - r.conic[1] * dx * dy;
+        real gw = sig > 0.0f ? 0.0f : std::exp(sig);
         if (r.opacity * gw < 1.0f / 255.0f) continue;
         int64_t idx = splat_index(x, y, q / k, np, c.up_w);
         uint64_t* slot = &c.buffer[(size_t)idx];
@@ -688,20 +699,20 @@ void resolve(const Ctx& c, float* color, float* depth, bool depth_only) {
     par_for(c.threads, (size_t)h, [&](size_t yb, size_t ye) {
         for (size_t y = yb; y < ye; ++y)
             for (int x = 0; x < w; ++x) {
-                float d = 1e9f, cr = 0, cg = 0, cb = 0;
+                real d = 1e9f, cr = 0, cg = 0, cb = 0;
                 for (int dx = 0; dx < ss; ++dx)
                     for (int dy = 0; dy < ss; ++dy)
                         for (int p = 0; p < np; ++p) {
                             int64_t i = splat_index(x * ss + dx, (int)y * ss + dy, p, np, c.up_w);
                             uint64_t v = c.buffer[(size_t)i];
-                            float vd = view_depth_from_key((v >> 36) & 0xFFFFFFFull, s.near_view_plane, s.far_view_plane);
+                            real vd = view_depth_from_key((v >> 36) & 0xFFFFFFFull, s.near_view_plane, s.far_view_plane);
                             d = gmin(d, view_to_ndc(vd, s.near_view_plane, s.far_view_plane));
                             if (depth_only) continue;
-                            cr += (float)((v >> 24) & 0xFFF) / 255.0f;
-                            cg += (float)((v >> 12) & 0xFFF) / 255.0f;
-                            cb += (float)(v & 0xFFF) / 255.0f;
+                            cr += (real)((v >> 24) & 0xFFF) / 255.0f;
+                            cg += (real)((v >> 12) & 0xFFF) / 255.0f;
+                            cb += (real)(v & 0xFFF) / 255.0f;
                         }
-                float inv = 1.0f / (float)(np * ss * ss);
+                real inv = 1.0f / (real)(np * ss * ss);
                 size_t idx = y * w + x;
                 if (!depth_only) {
                     color[3 * idx] = cr * inv;
@@ -757,7 +768,7 @@ oracle_ctx* oracle_create(const float* gaussians, uint64_t n, const gps_settings
         for (uint64_t i = (uint64_t)b * c->per_block; i < std::min<uint64_t>(n, (uint64_t)(b + 1) * c->per_block); ++i) {
             const Gaussian& g = c->g[i];
             M3 cov = scale_rot_to_cov(v3(g.scale[0], g.scale[1], g.scale[2]), v4(g.rot[0], g.rot[1], g.rot[2], g.rot[3]));
-            float d[3] = {cov.c[0].x, cov.c[1].y, cov.c[2].z};
+            float d[3] = {(float)cov.c[0].x, (float)cov.c[1].y, (float)cov.c[2].z};
             for (int k = 0; k < 3; ++k) {
                 float e = 3.0f * std::sqrt(d[k]);
                 float lo = g.mean[k] - e, hi = g.mean[k] + e;
@@ -807,7 +818,7 @@ void oracle_splat_workload(oracle_ctx* h, const gps_camera* cam, int frame_seed,
         for (size_t r = b; r < e; ++r) {
             uint32_t g = surv_gid[r];
             Record rec;
-            float ndc_z, det;
+            real ndc_z, det;
             V3 cov2d;
             if (geometry_record(c, f, g, rec, ndc_z, det, cov2d)) record_color(c, f, g, rec);
             else rec.mnx = rec.mny = rec.mxx = rec.mxy = 0;  // rejected here: no sample can land

@@ -13,15 +13,16 @@ import numpy as np
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "_build", "liboracle.so")
-_lib = None
+LIB64_PATH = os.path.join(_HERE, "_build", "liboracle64.so")  # the same estimator in double precision
+_libs = {}
 
 
-def lib():
-    global _lib
-    if _lib is None:
-        if not os.path.exists(LIB_PATH):
-            raise ImportError(f"{LIB_PATH} missing: run `make -C {_HERE}`")
-        L = ctypes.CDLL(LIB_PATH)
+def lib(fp64: bool = False):
+    if fp64 not in _libs:
+        path = LIB64_PATH if fp64 else LIB_PATH
+        if not os.path.exists(path):
+            raise ImportError(f"{path} missing: run `make -C {_HERE}`")
+        L = ctypes.CDLL(path)
         L.oracle_create.restype = c_void_p
         L.oracle_create.argtypes = [c_void_p, c_uint64, c_void_p, c_int]
         L.oracle_free.argtypes = [c_void_p]
@@ -41,8 +42,8 @@ def lib():
         L.oracle_splat_index.argtypes = [c_void_p, c_void_p, c_void_p, c_int, c_int, c_int, c_void_p]
         L.oracle_depth_key.argtypes = [c_void_p, c_int, c_float, c_float, c_void_p]
         L.oracle_rgb36.argtypes = [c_void_p, c_int, c_void_p]
-        _lib = L
-    return _lib
+        _libs[fp64] = L
+    return _libs[fp64]
 
 
 def _p(a: np.ndarray):
@@ -52,50 +53,52 @@ def _p(a: np.ndarray):
 class Oracle:
     """One scene + settings + frame state, rendered on the CPU with `threads` threads."""
 
-    def __init__(self, gaussians: np.ndarray, settings, threads: int = 1):
+    def __init__(self, gaussians: np.ndarray, settings, threads: int = 1, fp64: bool = False):
+        """fp64: the same estimator (same sample streams) in double precision."""
+        self._lib = lib(fp64)
         g = np.ascontiguousarray(gaussians, dtype=np.float32)
         self._g = g
         self.settings = settings
         self.n = g.shape[0]
-        self._h = lib().oracle_create(_p(g), g.shape[0], ctypes.addressof(settings), threads)
+        self._h = self._lib.oracle_create(_p(g), g.shape[0], ctypes.addressof(settings), threads)
 
     def render(self, cam):
         s = self.settings
         img = np.zeros((s.height, s.width, 3), np.float32)
         dep = np.zeros((s.height, s.width), np.float32)
-        lib().oracle_render_frame(self._h, ctypes.addressof(cam), _p(img), _p(dep))
+        self._lib.oracle_render_frame(self._h, ctypes.addressof(cam), _p(img), _p(dep))
         return img, dep
 
     def preprocess(self, cam, first_pass=True):
         counts = np.zeros(self.n, np.uint32)
         mask = np.zeros((self.n + 31) // 32, np.uint32)
         colors = np.zeros((self.n, 3), np.float32)
-        lib().oracle_preprocess(self._h, ctypes.addressof(cam), int(first_pass), _p(counts), _p(mask), _p(colors))
+        self._lib.oracle_preprocess(self._h, ctypes.addressof(cam), int(first_pass), _p(counts), _p(mask), _p(colors))
         return counts, mask, colors
 
     def splat_workload(self, cam, frame_seed, surv_gid, surv_start, points, clear=True):
         g = np.ascontiguousarray(surv_gid, np.uint32)
         st = np.ascontiguousarray(surv_start, np.uint32)
-        lib().oracle_splat_workload(self._h, ctypes.addressof(cam), frame_seed, _p(g), _p(st), g.size, points, int(clear))
+        self._lib.oracle_splat_workload(self._h, ctypes.addressof(cam), frame_seed, _p(g), _p(st), g.size, points, int(clear))
 
     def buffer(self):
-        out = np.zeros(lib().oracle_buffer_entries(self._h), np.uint64)
-        lib().oracle_get_buffer(self._h, _p(out))
+        out = np.zeros(self._lib.oracle_buffer_entries(self._h), np.uint64)
+        self._lib.oracle_get_buffer(self._h, _p(out))
         return out
 
     def hiz(self):
-        out = np.zeros(lib().oracle_hiz_size(self._h), np.float32)
-        lib().oracle_get_hiz(self._h, _p(out))
+        out = np.zeros(self._lib.oracle_hiz_size(self._h), np.float32)
+        self._lib.oracle_get_hiz(self._h, _p(out))
         return out
 
     def workload(self):
         pp = np.zeros(2, np.uint32)
         sv = c_uint32()
         tot = c_uint32()
-        lib().oracle_last_workload(self._h, _p(pp), byref(sv), byref(tot))
+        self._lib.oracle_last_workload(self._h, _p(pp), byref(sv), byref(tot))
         gid = np.zeros(sv.value, np.uint32)
         start = np.zeros(sv.value, np.uint32)
-        lib().oracle_get_survivors(self._h, _p(gid), _p(start))
+        self._lib.oracle_get_survivors(self._h, _p(gid), _p(start))
         return {"points_pass": pp, "survivors": sv.value, "total": tot.value, "surv_gid": gid, "surv_start": start}
 
     def blocks(self):
@@ -103,12 +106,12 @@ class Oracle:
         nodes = np.zeros(n * 6, np.float32)
         pb = c_uint32()
         cnt = c_uint32()
-        lib().oracle_get_blocks(self._h, _p(nodes), byref(pb), byref(cnt))
+        self._lib.oracle_get_blocks(self._h, _p(nodes), byref(pb), byref(cnt))
         return nodes[: cnt.value * 6].reshape(-1, 6), pb.value
 
     def close(self):
         if self._h:
-            lib().oracle_free(self._h)
+            self._lib.oracle_free(self._h)
             self._h = None
 
     def __del__(self):
