@@ -93,3 +93,53 @@ def test_tile_needs_half_scene():
         f32.tile([[0.0, 0.0], [10.0, 0.0]])
     assert e.value.status == 1
     f32.close()
+
+
+def test_paths_against_fp64_oracle():
+    """Same sample streams, 8-frame means: the FP32 path's arithmetic error is far below the
+    half format's, which stays below the 8-frame sampling noise (measured at 32 frames:
+    FP32 81 dB, half 41 dB, noise 37 dB)."""
+    import os
+    import sys
+
+    import torch
+
+    sys.path.insert(0, os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "oracle"))
+    import oracle
+
+    raw = synth.town(60000, seed=5)
+    g = synth.activate(raw)
+    s = gpsplat.default_settings(width=W, height=H, samples_per_pixel=4, max_number_of_points=4_000_000)
+    pose = synth.orbit(8, 30.0, 10.0)[3]
+    frames = 8
+    cams = lambda first: [gpsutil.cameras_for(s, [pose], first_frame=first + f)[0] for f in range(frames)]
+
+    def oracle_mean(first):
+        tot = np.zeros((H, W, 3))
+        for cam in cams(first):
+            o = oracle.Oracle(g, s, threads=os.cpu_count() or 1, fp64=True)
+            tot += o.render(cam)[0]
+            o.close()
+        return np.clip(tot / frames, 0, 1)
+
+    def gpu_mean(fmt):
+        scene = gpsplat.Scene.from_host(g, fmt, presorted=True)
+        r = gpsplat.Renderer(scene, s)
+        img = torch.empty((H, W, 3), device="cuda")
+        dep = torch.empty((H, W), device="cuda")
+        tot = np.zeros((H, W, 3))
+        for cam in cams(1):
+            r.reset(0)
+            r.render(cam, img.data_ptr(), dep.data_ptr(), 0)
+            torch.cuda.synchronize()
+            tot += img.cpu().numpy()
+        r.close()
+        scene.close()
+        return np.clip(tot / frames, 0, 1)
+
+    ref = oracle_mean(1)
+    noise = _psnr(oracle_mean(10001), ref)
+    fp32 = _psnr(gpu_mean(gpsplat.GPS_SCENE_FP32), ref)
+    half = _psnr(gpu_mean(gpsplat.GPS_SCENE_HALF), ref)
+    assert fp32 > 60.0, fp32
+    assert half > noise, (half, noise)
