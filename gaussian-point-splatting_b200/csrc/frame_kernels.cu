@@ -783,45 +783,6 @@ __global__ void __launch_bounds__(kSplatTile) splat_kernel(SplatArgs a) {
     }
 }
 
-// Warp-granular variant for the unbiased K-templated path: each warp walks 32-point subtiles
-// on its own and finds each point's owner by a binary search over the 256-entry survivor window
-// of its 256-point tile, read through L1 (neighbouring points share the search path, so the
-// loads broadcast).  No block barrier, so a slow warp does not hold up the rest of its block.
-#ifndef GPS_SPLAT_WARP_TILES
-#define GPS_SPLAT_WARP_TILES 0
-#endif
-
-template <int K>
-__global__ void __launch_bounds__(kSplatTile) splat_warp_kernel(SplatArgs a) {
-    const uint32_t points = a.counters->points;
-    const uint32_t survivors = a.counters->survivors;
-    const uint32_t lane = threadIdx.x & 31u;
-    const uint32_t warps = gridDim.x * (blockDim.x >> 5);
-    const uint32_t subtiles = (uint32_t)(((unsigned long long)points + 31) >> 5);
-    for (uint32_t st = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); st < subtiles; st += warps) {
-        const uint32_t p = (st << 5) + lane;
-        const uint32_t r0 = __ldg(a.tile_first_rank + (st << 5) / kSplatTile);
-        if (p >= points || r0 >= survivors || __ldg(a.surv_start + r0) > p) continue;
-        int lo = 0, hi = kSplatTile - 1;  // largest k with surv_start[r0 + k] <= p (past the end: +inf)
-        while (lo < hi) {
-            const int mid = (lo + hi + 1) >> 1;
-            const uint32_t r = r0 + (uint32_t)mid;
-            const uint32_t v = r < survivors ? __ldg(a.surv_start + r) : 0xFFFFFFFFu;
-            if (v <= p) lo = mid;
-            else hi = mid - 1;
-        }
-        const uint32_t g = __ldg(&a.surv_gid[r0 + lo]);
-        if (g >= a.n) continue;  // never, unless the workload is corrupt
-        const float4* rp = reinterpret_cast<const float4*>(a.records + g);
-        SplatRecord rec;
-        rec.a = __ldg(rp + 0);
-        rec.b = __ldg(rp + 1);
-        rec.c = __ldg(rp + 2);
-        rec.d = __ldg(reinterpret_cast<const uint4*>(rp + 3));
-        splat_point_unbiased_k<K>(p, rec, a.fc, a.frame_seed, a.buffer);
-    }
-}
-
 // ---------------------------------------------------------------------------------
 // Clear and resolve (gaussian_point_splatting.cu:484-548, 580-585)
 // ---------------------------------------------------------------------------------
@@ -1405,8 +1366,7 @@ template <int K>
 int splat_blocks_per_sm() {
     static int per_sm = 0;
     if (per_sm == 0) {
-        if constexpr (K > 0 && GPS_SPLAT_WARP_TILES) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, splat_warp_kernel<K>, kSplatTile, 0);
-        else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, splat_kernel<K>, kSplatTile, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, splat_kernel<K>, kSplatTile, 0);
         if (per_sm < 1) per_sm = 1;
     }
     return per_sm;
@@ -1427,11 +1387,9 @@ void launch_splat(const SplatArgs& a, int grid, int block, cudaStream_t stream) 
     if (g_num_sms == 0) splat_grid_size(kSplatTile);
     // a persistent grid: as many blocks as fit on the device at once
     if (a.fc.use_unbiased && a.fc.k_points == 4) {
-        if (GPS_SPLAT_WARP_TILES) splat_warp_kernel<4><<<g_num_sms * splat_blocks_per_sm<4>(), kSplatTile, 0, stream>>>(a);
-        else splat_kernel<4><<<g_num_sms * splat_blocks_per_sm<4>(), kSplatTile, 0, stream>>>(a);
+        splat_kernel<4><<<g_num_sms * splat_blocks_per_sm<4>(), kSplatTile, 0, stream>>>(a);
     } else if (a.fc.use_unbiased && a.fc.k_points == 1) {
-        if (GPS_SPLAT_WARP_TILES) splat_warp_kernel<1><<<g_num_sms * splat_blocks_per_sm<1>(), kSplatTile, 0, stream>>>(a);
-        else splat_kernel<1><<<g_num_sms * splat_blocks_per_sm<1>(), kSplatTile, 0, stream>>>(a);
+        splat_kernel<1><<<g_num_sms * splat_blocks_per_sm<1>(), kSplatTile, 0, stream>>>(a);
     } else {
         splat_kernel<0><<<grid, kSplatTile, 0, stream>>>(a);
     }
