@@ -1341,9 +1341,21 @@ struct gps_frame_loop {
     gps_renderer* r = nullptr;
     dptr<float> color[2], depth[2];
     dptr<float> taa_out;  // TAA writes here, then swaps with the current colour slot
-    dptr<uint8_t> u8;
+    dptr<uint8_t> u8[2];  // u8 frames alternate, so one can be read back while the next renders
+    int cur = 0;          // u8 slot of the last frame
+    cudaStream_t copy = nullptr;      // read-back stream of gps_frame_loop_read_async
+    cudaEvent_t framed = nullptr;     // end of the last frame, on the caller's stream
+    cudaEvent_t read_done[2] = {nullptr, nullptr};
+    bool reading[2] = {false, false};
     int progressive_frames = 0;
     mat4 prev_vp{};
+    ~gps_frame_loop() {
+        if (copy) cudaStreamSynchronize(copy);
+        if (copy) cudaStreamDestroy(copy);
+        if (framed) cudaEventDestroy(framed);
+        for (cudaEvent_t e : read_done)
+            if (e) cudaEventDestroy(e);
+    }
 };
 
 extern "C" {
@@ -1360,9 +1372,14 @@ gps_status gps_frame_loop_create(gps_renderer* r, gps_frame_loop** out) {
             GPS_CUDA(cudaMemset(l->color[i].get(), 0, px * 3 * sizeof(float)));
             GPS_CUDA(cudaMemset(l->depth[i].get(), 0, px * sizeof(float)));
         }
-        l->u8.reset(dev_alloc<uint8_t>(px * 3));
-        GPS_CUDA(cudaMemset(l->u8.get(), 0, px * 3));
+        for (int i = 0; i < 2; ++i) {
+            l->u8[i].reset(dev_alloc<uint8_t>(px * 3));
+            GPS_CUDA(cudaMemset(l->u8[i].get(), 0, px * 3));
+            GPS_CUDA(cudaEventCreateWithFlags(&l->read_done[i], cudaEventDisableTiming));
+        }
         l->taa_out.reset(dev_alloc<float>(px * 3));
+        GPS_CUDA(cudaStreamCreateWithFlags(&l->copy, cudaStreamNonBlocking));
+        GPS_CUDA(cudaEventCreateWithFlags(&l->framed, cudaEventDisableTiming));
     } catch (const CudaError& e) {
         return fail(GPS_ERR_OUT_OF_MEMORY, e.what());
     }
@@ -1381,6 +1398,12 @@ gps_status gps_frame_loop_step(gps_frame_loop* l, const gps_camera* cam, void* s
     if (st != GPS_OK) return st;
     const int w = r->s.width, h = r->s.height;
     mat4 view = mat4_from(cam->view), proj = mat4_from(cam->proj);
+    const int slot = 1 - l->cur;  // write the other u8 frame; wait if it is still being read back
+    if (l->reading[slot]) {
+        cudaStreamWaitEvent(as_stream(stream), l->read_done[slot], 0);
+        l->reading[slot] = false;
+    }
+    uint8_t* u8 = l->u8[slot].get();
     r->timer.mark(kStPost, as_stream(stream));
     r->frame_launches += 1;
     r->timer.launches[kStPost] += 1;
@@ -1388,16 +1411,17 @@ gps_status gps_frame_loop_step(gps_frame_loop* l, const gps_camera* cam, void* s
         l->progressive_frames++;
         mat4 model = affine_inverse(view);
         mat4 delta = mat4_mul(mat4_mul(l->prev_vp, model), inverse4(proj));
-        launch_taa(l->u8.get(), l->taa_out.get(), l->color[a].get(), l->color[b].get(), l->depth[a].get(),
+        launch_taa(u8, l->taa_out.get(), l->color[a].get(), l->color[b].get(), l->depth[a].get(),
                    l->depth[b].get(), delta, 0.9f, w, h, l->progressive_frames, as_stream(stream));
         std::swap(l->color[a], l->taa_out);
     } else {
         if (cam->camera_moved || r->s.accumulation_mode == GPS_ACCUM_NONE) l->progressive_frames = 1;
         else l->progressive_frames++;
-        launch_progressive(l->u8.get(), l->color[a].get(), l->color[b].get(), w, h, l->progressive_frames,
+        launch_progressive(u8, l->color[a].get(), l->color[b].get(), w, h, l->progressive_frames,
                            as_stream(stream));
     }
     r->timer.mark(-1, as_stream(stream));
+    l->cur = slot;
     l->prev_vp = mat4_mul(proj, view);
     cudaError_t e = cudaGetLastError();
     return e == cudaSuccess ? GPS_OK : fail(GPS_ERR_CUDA, cudaGetErrorString(e));
@@ -1406,15 +1430,34 @@ gps_status gps_frame_loop_step(gps_frame_loop* l, const gps_camera* cam, void* s
 gps_status gps_frame_loop_read(gps_frame_loop* l, uint8_t* host_rgb, void* stream) {
     if (!l || !host_rgb) return fail(GPS_ERR_INVALID_ARGUMENT, "null argument");
     const size_t bytes = (size_t)l->r->s.width * l->r->s.height * 3;
-    cudaError_t e = cudaMemcpyAsync(host_rgb, l->u8.get(), bytes, cudaMemcpyDeviceToHost, as_stream(stream));
+    cudaError_t e = cudaMemcpyAsync(host_rgb, l->u8[l->cur].get(), bytes, cudaMemcpyDeviceToHost, as_stream(stream));
     if (e == cudaSuccess) e = cudaStreamSynchronize(as_stream(stream));
+    return e == cudaSuccess ? GPS_OK : fail(GPS_ERR_CUDA, cudaGetErrorString(e));
+}
+
+gps_status gps_frame_loop_read_async(gps_frame_loop* l, uint8_t* host_rgb, void* stream) {
+    if (!l || !host_rgb) return fail(GPS_ERR_INVALID_ARGUMENT, "null argument");
+    const size_t bytes = (size_t)l->r->s.width * l->r->s.height * 3;
+    const int slot = l->cur;
+    cudaEventRecord(l->framed, as_stream(stream));
+    cudaStreamWaitEvent(l->copy, l->framed, 0);
+    cudaError_t e = cudaMemcpyAsync(host_rgb, l->u8[slot].get(), bytes, cudaMemcpyDeviceToHost, l->copy);
+    if (e == cudaSuccess) e = cudaEventRecord(l->read_done[slot], l->copy);
+    l->reading[slot] = true;
+    return e == cudaSuccess ? GPS_OK : fail(GPS_ERR_CUDA, cudaGetErrorString(e));
+}
+
+gps_status gps_frame_loop_read_wait(gps_frame_loop* l) {
+    if (!l) return fail(GPS_ERR_INVALID_ARGUMENT, "null argument");
+    cudaError_t e = cudaStreamSynchronize(l->copy);
+    l->reading[0] = l->reading[1] = false;
     return e == cudaSuccess ? GPS_OK : fail(GPS_ERR_CUDA, cudaGetErrorString(e));
 }
 
 gps_status gps_frame_loop_buffers(gps_frame_loop* l, int32_t slot, const uint8_t** d_u8, const float** d_color,
                                   const float** d_depth) {
     if (!l || slot < 0 || slot > 2) return fail(GPS_ERR_INVALID_ARGUMENT, "bad argument");
-    if (d_u8) *d_u8 = l->u8.get();
+    if (d_u8) *d_u8 = l->u8[l->cur].get();
     if (slot == 2) {
         // resolved colour of the last frame before TAA blended it (TAA mode only)
         if (d_color) *d_color = l->taa_out.get();

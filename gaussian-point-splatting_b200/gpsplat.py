@@ -191,6 +191,8 @@ _SIGNATURES = [
     ("gps_frame_loop_free", None, [c_void_p]),
     ("gps_frame_loop_step", c_int32, [c_void_p, POINTER(Camera), c_void_p]),
     ("gps_frame_loop_read", c_int32, [c_void_p, c_void_p, c_void_p]),
+    ("gps_frame_loop_read_async", c_int32, [c_void_p, c_void_p, c_void_p]),
+    ("gps_frame_loop_read_wait", c_int32, [c_void_p]),
     ("gps_frame_loop_buffers", c_int32, [c_void_p, c_int32, POINTER(c_void_p), POINTER(c_void_p), POINTER(c_void_p)]),
     ("gps_camera_path_load", c_int32, [c_char_p, POINTER(c_void_p)]),
     ("gps_camera_path_count", c_int32, [c_void_p]),
@@ -539,6 +541,13 @@ class FrameLoop:
             out = np.empty((s.height, s.width, 3), np.uint8)
         _check(load_library().gps_frame_loop_read(self._h, out.ctypes.data, c_void_p(stream)))
         return out
+
+    def read_async(self, out: np.ndarray, stream: int = 0):
+        """Starts copying the last frame to `out` (pinned, untouched until read_wait)."""
+        _check(load_library().gps_frame_loop_read_async(self._h, out.ctypes.data, c_void_p(stream)))
+
+    def read_wait(self):
+        _check(load_library().gps_frame_loop_read_wait(self._h))
 
     def buffers(self, slot: int):
         """(u8 image, colour, depth) device pointers of ping-pong slot 0 or 1."""

@@ -319,6 +319,13 @@ void gps_frame_loop_free(gps_frame_loop* l);
 gps_status gps_frame_loop_step(gps_frame_loop* l, const gps_camera* cam, void* stream);
 /* Copies the last u8 RGB frame (W*H*3 bytes) to host memory. */
 gps_status gps_frame_loop_read(gps_frame_loop* l, uint8_t* host_rgb, void* stream);
+/* The same copy without waiting: it runs on the loop's own copy stream once the last frame on
+ * `stream` is done, while the next frames render (u8 frames alternate between two buffers; a
+ * step waits only if it would overwrite a frame still being copied).  host_rgb should be pinned
+ * and must stay untouched until gps_frame_loop_read_wait returns. */
+gps_status gps_frame_loop_read_async(gps_frame_loop* l, uint8_t* host_rgb, void* stream);
+/* Waits for every copy started by gps_frame_loop_read_async. */
+gps_status gps_frame_loop_read_wait(gps_frame_loop* l);
 /* Device buffers of ping-pong slot `slot` (0 or 1): frame f renders its colour into slot
  * f % 2 and its depth into slot 1 - f % 2 (render_server.cu:87-92).  Slot 2 (TAA mode):
  * the last frame's resolved colour before TAA blended it (no depth). */

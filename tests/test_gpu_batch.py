@@ -107,3 +107,31 @@ def test_reset_makes_next_frame_a_fresh_render():
     assert np.array_equal(dep.cpu().numpy().view(np.uint32), want_dep.view(np.uint32))
     r.close()
     scene.close()
+
+
+def test_frame_loop_async_readback_matches_blocking_read():
+    """gps_frame_loop_read_async alternates two u8 frames; the frames it reads back equal the
+    blocking read of the same frames on an identical loop."""
+    import torch
+
+    ply = gpsutil.cached_ply("town60k", lambda: synth.town(60000, seed=5))
+    scene = gpsplat.Scene.from_ply(ply)
+    s = gpsplat.default_settings(width=320, height=180, samples_per_pixel=2, max_number_of_points=4_000_000,
+                                 accumulation_mode=gpsplat.GPS_ACCUM_TAA)
+    cams = gpsutil.cameras_for(s, synth.orbit(5, 30.0, 10.0))
+    ra, rb = gpsplat.Renderer(scene, s), gpsplat.Renderer(scene, s)
+    la, lb = gpsplat.FrameLoop(ra), gpsplat.FrameLoop(rb)
+    want = []
+    for c in cams:
+        la.step(c)
+        want.append(la.read().copy())
+    host = [torch.empty((180, 320, 3), dtype=torch.uint8, pin_memory=True) for _ in range(2)]
+    for i, c in enumerate(cams):
+        lb.step(c)
+        lb.read_async(host[i % 2].numpy())
+    lb.read_wait()
+    n = len(cams)
+    assert np.array_equal(host[(n - 1) % 2].numpy(), want[-1])
+    assert np.array_equal(host[(n - 2) % 2].numpy(), want[-2])
+    for obj in (la, lb, ra, rb, scene):
+        obj.close()
