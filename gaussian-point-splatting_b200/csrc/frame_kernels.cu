@@ -566,6 +566,11 @@ __device__ __forceinline__ void splat_point_biased(uint32_t point, const SplatRe
 #ifndef GPS_SPLAT_PIPELINE
 #define GPS_SPLAT_PIPELINE 1
 #endif
+// 1: a sample's in-tile Morton code comes from a 64-entry shared-memory table of spread 6-bit
+// coordinates (two table loads) instead of two 4-step bit spreads; the codes are identical.
+#ifndef GPS_SPLAT_MORTON_LUT
+#define GPS_SPLAT_MORTON_LUT 0
+#endif
 constexpr int kSplatBatch = GPS_SPLAT_BATCH;
 
 __device__ __forceinline__ void splat_point_unbiased(uint32_t point, const SplatRecord& rec, const FrameConst& fc,
@@ -649,6 +654,7 @@ struct SampleConst {
     vec3 conic;
     int minx, miny, maxx, maxy;
     int tiles_per_row, passes;
+    const uint32_t* spread;  // shared-memory Morton table (GPS_SPLAT_MORTON_LUT)
 };
 
 __device__ __forceinline__ bool draw_sample(u32x2& seed, const SampleConst& c, int p, uint32_t& slot) {
@@ -667,7 +673,11 @@ __device__ __forceinline__ bool draw_sample(u32x2& seed, const SampleConst& c, i
     const vec2 delta = make_v2(c.pixel_mean.x - pixel.x, c.pixel_mean.y - pixel.y);
     const bool inside = (x >= c.minx) & (x < c.maxx) & (y >= c.miny) & (y < c.maxy);
     const float alpha = c.opacity * gaussian_value(c.conic, delta);
+#if GPS_SPLAT_MORTON_LUT
+    const uint32_t code = c.spread[x & (kTileSize - 1)] | (c.spread[y & (kTileSize - 1)] << 1);
+#else
     const uint32_t code = morton_encode((uint32_t)(x & (kTileSize - 1)), (uint32_t)(y & (kTileSize - 1)));
+#endif
     const uint32_t tile = (uint32_t)((y >> kTileBits) * c.tiles_per_row + (x >> kTileBits));
     slot = (tile * (uint32_t)(kTileSize * kTileSize) + code) * (uint32_t)c.passes + (uint32_t)p;
     return inside & !(alpha < 1.0f / 255.0f);
@@ -675,9 +685,11 @@ __device__ __forceinline__ bool draw_sample(u32x2& seed, const SampleConst& c, i
 
 template <int K>
 __device__ __forceinline__ void splat_point_unbiased_k(uint32_t point, const SplatRecord& rec, const FrameConst& fc,
-                                                       int frame_seed, uint64_t* __restrict__ buffer) {
+                                                       int frame_seed, uint64_t* __restrict__ buffer,
+                                                       const uint32_t* spread) {
     u32x2 seed = make_seed(point, (uint32_t)frame_seed);
     SampleConst c;
+    c.spread = spread;
     c.pixel_mean = make_v2(rec.a.x, rec.a.y);
     c.c0 = rec.a.z;
     c.c1 = rec.a.w;
@@ -745,6 +757,8 @@ __device__ __forceinline__ void splat_point_unbiased_k(uint32_t point, const Spl
 template <int K>
 __global__ void __launch_bounds__(kSplatTile) splat_kernel(SplatArgs a) {
     __shared__ uint32_t s_start[kSplatTile];
+    __shared__ uint32_t s_spread[kTileSize];
+    if (GPS_SPLAT_MORTON_LUT && threadIdx.x < kTileSize) s_spread[threadIdx.x] = morton_spread(threadIdx.x);
     const uint32_t points = a.counters->points;
     const uint32_t survivors = a.counters->survivors;
     for (uint32_t tile = blockIdx.x; (unsigned long long)tile * kSplatTile < points; tile += gridDim.x) {
@@ -772,7 +786,7 @@ __global__ void __launch_bounds__(kSplatTile) splat_kernel(SplatArgs a) {
                 rec.c = __ldg(rp + 2);
                 rec.d = __ldg(reinterpret_cast<const uint4*>(rp + 3));
                 if constexpr (K > 0) {
-                    splat_point_unbiased_k<K>(p, rec, a.fc, a.frame_seed, a.buffer);
+                    splat_point_unbiased_k<K>(p, rec, a.fc, a.frame_seed, a.buffer, s_spread);
                 } else {
                     if (a.fc.use_unbiased) splat_point_unbiased(p, rec, a.fc, a.frame_seed, a.buffer);
                     else splat_point_biased(p, rec, a.fc, a.frame_seed, a.buffer);

@@ -20,6 +20,7 @@
 #include <vector>
 #include "../../include/gps_b200.h"
 #include "frame_kernels.h"
+#include "host_images.hpp"
 #include "host_io.hpp"
 
 using namespace gps;
@@ -1343,6 +1344,7 @@ struct gps_frame_loop {
     dptr<float> taa_out;  // TAA writes here, then swaps with the current colour slot
     dptr<uint8_t> u8[2];  // u8 frames alternate, so one can be read back while the next renders
     int cur = 0;          // u8 slot of the last frame
+    int last_color = 0;   // colour slot the last frame resolved (and accumulated) into
     cudaStream_t copy = nullptr;      // read-back stream of gps_frame_loop_read_async
     cudaEvent_t framed = nullptr;     // end of the last frame, on the caller's stream
     cudaEvent_t read_done[2] = {nullptr, nullptr};
@@ -1422,6 +1424,7 @@ gps_status gps_frame_loop_step(gps_frame_loop* l, const gps_camera* cam, void* s
     }
     r->timer.mark(-1, as_stream(stream));
     l->cur = slot;
+    l->last_color = a;
     l->prev_vp = mat4_mul(proj, view);
     cudaError_t e = cudaGetLastError();
     return e == cudaSuccess ? GPS_OK : fail(GPS_ERR_CUDA, cudaGetErrorString(e));
@@ -1466,6 +1469,87 @@ gps_status gps_frame_loop_buffers(gps_frame_loop* l, int32_t slot, const uint8_t
     }
     if (d_color) *d_color = l->color[slot].get();
     if (d_depth) *d_depth = l->depth[slot].get();
+    return GPS_OK;
+}
+
+// ---- evaluation workflow --------------------------------------------------------------
+
+gps_status gps_write_png(const char* path, const uint8_t* host_rgb, int32_t width, int32_t height, int32_t flip_rows) {
+    if (!path || !host_rgb || width <= 0 || height <= 0) return fail(GPS_ERR_INVALID_ARGUMENT, "bad argument");
+    const int rc = write_png(path, host_rgb, width, height, flip_rows != 0);
+    if (rc == 3) return fail(GPS_ERR_IO, std::string("cannot write ") + path);
+    return rc ? fail(GPS_ERR_INVALID_ARGUMENT, "PNG encoding failed") : GPS_OK;
+}
+
+gps_status gps_write_pfm(const char* path, const float* host_rgb, int32_t width, int32_t height) {
+    if (!path || !host_rgb || width <= 0 || height <= 0) return fail(GPS_ERR_INVALID_ARGUMENT, "bad argument");
+    return write_pfm(path, host_rgb, width, height) ? fail(GPS_ERR_IO, std::string("cannot write ") + path) : GPS_OK;
+}
+
+gps_status gps_frame_loop_export_pfm(gps_frame_loop* l, const char* path, void* stream) {
+    if (!l || !path) return fail(GPS_ERR_INVALID_ARGUMENT, "null argument");
+    const int w = l->r->s.width, h = l->r->s.height;
+    const size_t n = (size_t)w * h * 3;
+    std::vector<float> host(n);
+    cudaError_t e = cudaMemcpyAsync(host.data(), l->color[l->last_color].get(), n * sizeof(float),
+                                    cudaMemcpyDeviceToHost, as_stream(stream));
+    if (e == cudaSuccess) e = cudaStreamSynchronize(as_stream(stream));
+    if (e != cudaSuccess) return fail(GPS_ERR_CUDA, cudaGetErrorString(e));
+    // export_pfm_from_buffer: colour / float(numFrames), per component
+    const float frames = (float)(l->progressive_frames > 0 ? l->progressive_frames : 1);
+    for (size_t i = 0; i < n; ++i) host[i] = host[i] / frames;
+    return gps_write_pfm(path, host.data(), w, h);
+}
+
+gps_status gps_evaluate(gps_frame_loop* l, const gps_camera_path* path, const char* out_dir,
+                        const int32_t* spp_targets, int32_t num_targets, int32_t max_eval_count,
+                        int32_t first_frame, int32_t write_pfm_too, int32_t* frames_rendered) {
+    if (!l || !path || !out_dir) return fail(GPS_ERR_INVALID_ARGUMENT, "null argument");
+    static const int32_t kDefaultTargets[] = {1, 4, 16, 64, 256, 1024};  // main.cu:72
+    if (!spp_targets) {
+        spp_targets = kDefaultTargets;
+        num_targets = 6;
+    }
+    if (num_targets <= 0 || max_eval_count < 0) return fail(GPS_ERR_INVALID_ARGUMENT, "bad evaluation targets");
+    for (int i = 0; i < num_targets; ++i)
+        if (spp_targets[i] < 1 || (i > 0 && spp_targets[i] <= spp_targets[i - 1]))
+            return fail(GPS_ERR_INVALID_ARGUMENT, "spp targets must be positive and increasing");
+    if (!make_dirs(out_dir)) return fail(GPS_ERR_IO, std::string("cannot create ") + out_dir);
+    gps_renderer* r = l->r;
+    const int w = r->s.width, h = r->s.height;
+    std::vector<uint8_t> rgb((size_t)w * h * 3);
+    const int cameras = gps_camera_path_count(path);
+    int frame = first_frame, rendered = 0;
+    // main.cu:95-107: after camera c finishes, the run ends if c >= count - 1 or c >= max_eval_count
+    for (int c = 0; c < cameras; ++c) {
+        gps_camera_state st;
+        gps_status rc = gps_camera_path_get(path, c, &st);
+        if (rc != GPS_OK) return rc;
+        gps_settings s = r->s;
+        int32_t can_override = 0;  // the resolution is fixed once the renderer exists
+        std::string name = st.img_name[0] ? std::string(st.img_name) : "cam" + std::to_string(c);
+        int next = 0;
+        for (int f = 1; f <= spp_targets[num_targets - 1]; ++f, ++frame) {
+            gps_camera cam;
+            rc = gps_camera_from_state(&st, &s, 0, &can_override, frame, &cam);
+            if (rc != GPS_OK) return rc;
+            cam.camera_moved = f == 1;
+            rc = gps_frame_loop_step(l, &cam, nullptr);
+            if (rc != GPS_OK) return rc;
+            ++rendered;
+            if (f != spp_targets[next]) continue;
+            char suffix[16];
+            std::snprintf(suffix, sizeof(suffix), "_spp%04d", f);
+            const std::string stem = std::string(out_dir) + "/" + name + suffix;
+            rc = gps_frame_loop_read(l, rgb.data(), nullptr);
+            if (rc == GPS_OK) rc = gps_write_png((stem + ".png").c_str(), rgb.data(), w, h, 1);
+            if (rc == GPS_OK && write_pfm_too) rc = gps_frame_loop_export_pfm(l, (stem + ".pfm").c_str(), nullptr);
+            if (rc != GPS_OK) return rc;
+            ++next;
+        }
+        if (c >= cameras - 1 || c >= max_eval_count) break;
+    }
+    if (frames_rendered) *frames_rendered = rendered;
     return GPS_OK;
 }
 

@@ -194,6 +194,11 @@ _SIGNATURES = [
     ("gps_frame_loop_read_async", c_int32, [c_void_p, c_void_p, c_void_p]),
     ("gps_frame_loop_read_wait", c_int32, [c_void_p]),
     ("gps_frame_loop_buffers", c_int32, [c_void_p, c_int32, POINTER(c_void_p), POINTER(c_void_p), POINTER(c_void_p)]),
+    ("gps_write_png", c_int32, [c_char_p, c_void_p, c_int32, c_int32, c_int32]),
+    ("gps_write_pfm", c_int32, [c_char_p, c_void_p, c_int32, c_int32]),
+    ("gps_frame_loop_export_pfm", c_int32, [c_void_p, c_char_p, c_void_p]),
+    ("gps_evaluate", c_int32, [c_void_p, c_void_p, c_char_p, POINTER(c_int32), c_int32, c_int32, c_int32, c_int32,
+                               POINTER(c_int32)]),
     ("gps_camera_path_load", c_int32, [c_char_p, POINTER(c_void_p)]),
     ("gps_camera_path_count", c_int32, [c_void_p]),
     ("gps_camera_path_get", c_int32, [c_void_p, c_int32, POINTER(CameraState)]),
@@ -555,6 +560,23 @@ class FrameLoop:
         _check(load_library().gps_frame_loop_buffers(self._h, slot, byref(u8), byref(col), byref(dep)))
         return u8.value, col.value, dep.value
 
+    def export_pfm(self, path: str, stream: int = 0):
+        """The running mean of the last frame's colour buffer as a PFM (export_pfm_from_buffer)."""
+        _check(load_library().gps_frame_loop_export_pfm(self._h, path.encode(), c_void_p(stream)))
+
+    def evaluate(self, cameras: "CameraPath", out_dir: str, spp_targets=None, max_eval_count: int = 40,
+                 first_frame: int = 0, write_pfm: bool = False) -> int:
+        """The evaluation-screenshot run (main.cu:72-120): <out_dir>/<img_name>_spp%04d.png per
+        camera and spp target.  Returns the number of frames rendered."""
+        tgt, n = None, 0
+        if spp_targets is not None:
+            n = len(spp_targets)
+            tgt = (c_int32 * n)(*spp_targets)
+        frames = c_int32(0)
+        _check(load_library().gps_evaluate(self._h, cameras._h, out_dir.encode(), tgt, n, max_eval_count,
+                                           first_frame, int(write_pfm), byref(frames)))
+        return frames.value
+
     def close(self):
         if self._h:
             load_library().gps_frame_loop_free(self._h)
@@ -565,6 +587,18 @@ class FrameLoop:
             self.close()
         except Exception:
             pass
+
+
+def write_png(path: str, rgb: np.ndarray, flip_rows: bool = False):
+    """8-bit RGB (H, W, 3) to PNG (stbi_write_png)."""
+    rgb = np.ascontiguousarray(rgb, dtype=np.uint8)
+    _check(load_library().gps_write_png(path.encode(), rgb.ctypes.data, rgb.shape[1], rgb.shape[0], int(flip_rows)))
+
+
+def write_pfm(path: str, rgb: np.ndarray):
+    """float32 RGB (H, W, 3) to PFM (write_pfm)."""
+    rgb = np.ascontiguousarray(rgb, dtype=np.float32)
+    _check(load_library().gps_write_pfm(path.encode(), rgb.ctypes.data, rgb.shape[1], rgb.shape[0]))
 
 
 def splitmix64(x: np.ndarray) -> np.ndarray:

@@ -332,6 +332,27 @@ gps_status gps_frame_loop_read_wait(gps_frame_loop* l);
 gps_status gps_frame_loop_buffers(gps_frame_loop* l, int32_t slot, const uint8_t** d_u8, const float** d_color,
                                   const float** d_depth);
 
+/* ---- evaluation workflow (main.cu:72-120, render_server.cu:162-315) ----------------- */
+/* 8-bit RGB PNG (stbi_write_png in save_image_to_disk); flip_rows != 0 writes the last row
+ * first, as save_image_to_disk does with the frame it reads back. */
+gps_status gps_write_png(const char* path, const uint8_t* host_rgb, int32_t width, int32_t height, int32_t flip_rows);
+/* write_pfm: "PF\n<w> <h>\n-1.0\n", then the W*H*3 floats in memory order. */
+gps_status gps_write_pfm(const char* path, const float* host_rgb, int32_t width, int32_t height);
+/* export_pfm_from_buffer: the colour buffer the last step resolved into, divided by the
+ * accumulated frame count (the running mean in progressive mode), as a PFM file. */
+gps_status gps_frame_loop_export_pfm(gps_frame_loop* l, const char* path, void* stream);
+/* The --create-evaluation-screenshots run without the viewer: for each camera of the path
+ * (0 .. min(count - 1, max_eval_count), the reference's stopping rule), progressive frames
+ * restart at 1 (camera_moved), and after frame t of each spp target t the u8 frame is written
+ * to <out_dir>/<img_name>_spp%04d.png (rows flipped, as the reference saves them; "cam<i>"
+ * when the camera has no name), plus a .pfm of the running mean when write_pfm != 0.
+ * spp_targets NULL = {1, 4, 16, 64, 256, 1024}; targets must increase.  Frame numbers
+ * (seeds, ping-pong slots) run on from first_frame across cameras.  Renders on the default
+ * stream and returns when the files are written. */
+gps_status gps_evaluate(gps_frame_loop* l, const gps_camera_path* path, const char* out_dir,
+                        const int32_t* spp_targets, int32_t num_targets, int32_t max_eval_count,
+                        int32_t first_frame, int32_t write_pfm, int32_t* frames_rendered);
+
 /* ---- cameras (camera_loader.cu:62-150, main.cu:141-157, camera.cpp:88-156) ---------- */
 gps_status gps_camera_path_load(const char* json_path, gps_camera_path** out);
 int32_t gps_camera_path_count(const gps_camera_path* p);

@@ -231,3 +231,30 @@ def cached_ply(name: str, make) -> str:
         raw.write_ply(tmp)
         os.replace(tmp, p)
     return p
+
+
+def decode_png(data: bytes):
+    """A minimal PNG reader for 8-bit RGB, filter type 0 (what gps_write_png writes)."""
+    import struct
+    import zlib
+
+    assert data[:8] == b"\x89PNG\r\n\x1a\n"
+    pos, idat, ihdr, types = 8, b"", None, []
+    while pos < len(data):
+        (n,) = struct.unpack(">I", data[pos:pos + 4])
+        kind, body = data[pos + 4:pos + 8], data[pos + 8:pos + 8 + n]
+        (crc,) = struct.unpack(">I", data[pos + 8 + n:pos + 12 + n])
+        assert zlib.crc32(kind + body) == crc, kind
+        types.append(kind)
+        if kind == b"IHDR":
+            ihdr = struct.unpack(">IIBBBBB", body)
+        elif kind == b"IDAT":
+            idat += body
+        pos += 12 + n
+    assert types[0] == b"IHDR" and types[-1] == b"IEND"
+    w, h, depth, colour, _, _, interlace = ihdr
+    assert (depth, colour, interlace) == (8, 2, 0)
+    raw = np.frombuffer(zlib.decompress(idat), np.uint8).reshape(h, 1 + 3 * w)
+    assert (raw[:, 0] == 0).all()
+    return raw[:, 1:].reshape(h, w, 3)
+

@@ -13,6 +13,7 @@ import numpy as np
 import pytest
 
 import gpsplat
+import gpsutil
 import synth
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
@@ -238,3 +239,26 @@ def test_invalid_renderer_settings_are_rejected_without_gpu():
     assert lib.gps_renderer_create(None, ctypes.byref(s), ctypes.byref(r)) == 1
     assert lib.gps_render_frame(None, None, None, None, None) == 1
     assert lib.gps_post_taa(None, None, None, None, None, None, None, 0.9, 1, 1, 1, None) == 1
+
+
+def test_png_writer_roundtrip_and_flip(tmp_path):
+    rng = np.random.default_rng(3)
+    img = rng.integers(0, 256, size=(37, 53, 3), dtype=np.uint8)
+    p = str(tmp_path / "a.png")
+    gpsplat.write_png(p, img)
+    assert np.array_equal(gpsutil.decode_png(open(p, "rb").read()), img)
+    gpsplat.write_png(p, img, flip_rows=True)  # save_image_to_disk's row swap
+    assert np.array_equal(gpsutil.decode_png(open(p, "rb").read()), img[::-1])
+    with pytest.raises(gpsplat.GpsError) as e:
+        gpsplat.write_png(str(tmp_path / "missing_dir" / "a.png"), img)
+    assert e.value.status == 2
+
+
+def test_pfm_writer_layout(tmp_path):
+    img = np.arange(4 * 6 * 3, dtype=np.float32).reshape(4, 6, 3) / 7.0
+    p = str(tmp_path / "a.pfm")
+    gpsplat.write_pfm(p, img)
+    data = open(p, "rb").read()
+    head = b"PF\n6 4\n-1.0\n"
+    assert data[:len(head)] == head
+    assert np.array_equal(np.frombuffer(data[len(head):], "<f4").reshape(4, 6, 3), img)
