@@ -776,29 +776,34 @@ __device__ __forceinline__ void splat_point_unbiased_k(uint32_t point, const Spl
 #endif
 }
 
+// 1: the tile loop double-buffers its survivor-start table: tile t+1's table loads are issued
+// before tile t's points are splatted (and tile t+2's first rank one tile earlier still), so
+// no dependent global load sits between two tiles; one barrier per tile either way.
+#ifndef GPS_SPLAT_PREFETCH
+#define GPS_SPLAT_PREFETCH 0
+#endif
+
 // K > 0: unbiased splatting with K points per thread per pass; K = 0: any other setting.
 template <int K>
+#if GPS_SPLAT_PREFETCH
+__global__ void __launch_bounds__(kSplatTile, 4) splat_kernel(SplatArgs a) {
+#else
 __global__ void __launch_bounds__(kSplatTile) splat_kernel(SplatArgs a) {
+#endif
     pdl_enter();
-    __shared__ uint32_t s_start[kSplatTile];
+    __shared__ uint32_t s_start[GPS_SPLAT_PREFETCH ? 2 : 1][kSplatTile];
     __shared__ uint32_t s_spread[kTileSize];
     if (GPS_SPLAT_MORTON_LUT && threadIdx.x < kTileSize) s_spread[threadIdx.x] = morton_spread(threadIdx.x);
     const uint32_t points = a.counters->points;
     const uint32_t survivors = a.counters->survivors;
-    for (uint32_t tile = blockIdx.x; (unsigned long long)tile * kSplatTile < points; tile += gridDim.x) {
-        const uint32_t p0 = tile * kSplatTile;
-        const uint32_t r0 = a.tile_first_rank[tile];
-        {
-            uint32_t r = r0 + threadIdx.x;
-            s_start[threadIdx.x] = (r0 < survivors && r < survivors) ? a.surv_start[r] : 0xFFFFFFFFu;
-        }
-        __syncthreads();
+    // splats point p0 + threadIdx.x of a tile whose survivor starts are in `starts`
+    auto splat_tile_point = [&](uint32_t p0, uint32_t r0, const uint32_t* starts) {
         const uint32_t p = p0 + threadIdx.x;
-        if (p < points && s_start[0] <= p) {
-            int lo = 0, hi = kSplatTile - 1;  // largest k with s_start[k] <= p
+        if (p < points && starts[0] <= p) {
+            int lo = 0, hi = kSplatTile - 1;  // largest k with starts[k] <= p
             while (lo < hi) {
                 int mid = (lo + hi + 1) >> 1;
-                if (s_start[mid] <= p) lo = mid;
+                if (starts[mid] <= p) lo = mid;
                 else hi = mid - 1;
             }
             const uint32_t g = __ldg(&a.surv_gid[r0 + lo]);
@@ -817,8 +822,48 @@ __global__ void __launch_bounds__(kSplatTile) splat_kernel(SplatArgs a) {
                 }
             }
         }
+    };
+    auto start_of = [&](uint32_t r0) {
+        const uint32_t r = r0 + threadIdx.x;
+        return (r0 < survivors && r < survivors) ? a.surv_start[r] : 0xFFFFFFFFu;
+    };
+#if GPS_SPLAT_PREFETCH
+    uint32_t tile = blockIdx.x;
+    if ((unsigned long long)tile * kSplatTile >= points) return;  // uniform over the block
+    uint32_t r0 = a.tile_first_rank[tile];
+    s_start[0][threadIdx.x] = start_of(r0);
+    uint32_t next = tile + gridDim.x;
+    uint32_t next_r0 = (unsigned long long)next * kSplatTile < points ? a.tile_first_rank[next] : 0u;
+    __syncthreads();
+    int buf = 0;
+    for (;;) {
+        const bool has_next = (unsigned long long)next * kSplatTile < points;
+        const uint32_t after = next + gridDim.x;
+        uint32_t next_start = 0xFFFFFFFFu, after_r0 = 0u;
+        if (has_next) {
+            next_start = start_of(next_r0);
+            if ((unsigned long long)after * kSplatTile < points) after_r0 = a.tile_first_rank[after];
+        }
+        splat_tile_point(tile * kSplatTile, r0, s_start[buf]);
+        if (!has_next) break;
+        // s_start[buf ^ 1] was last read before the previous barrier
+        s_start[buf ^ 1][threadIdx.x] = next_start;
+        __syncthreads();
+        buf ^= 1;
+        tile = next;
+        r0 = next_r0;
+        next = after;
+        next_r0 = after_r0;
+    }
+#else
+    for (uint32_t tile = blockIdx.x; (unsigned long long)tile * kSplatTile < points; tile += gridDim.x) {
+        const uint32_t r0 = a.tile_first_rank[tile];
+        s_start[0][threadIdx.x] = start_of(r0);
+        __syncthreads();
+        splat_tile_point(tile * kSplatTile, r0, s_start[0]);
         __syncthreads();
     }
+#endif
 }
 
 // ---------------------------------------------------------------------------------
