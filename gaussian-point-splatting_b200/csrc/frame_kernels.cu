@@ -159,8 +159,10 @@ __global__ void __launch_bounds__(256) block_cull_kernel(BlockView b, FrameConst
 // Chunks of 32 Gaussians (one survivor-mask word each) that contain an unculled block, appended
 // warp by warp; culled chunks get their mask word zeroed here, since the preprocess skips them.
 __global__ void __launch_bounds__(256) visible_chunks_kernel(BlockView b, uint32_t n, uint32_t* __restrict__ list,
-                                                             uint32_t* __restrict__ mask_cur) {
+                                                             uint32_t* mask_cur, uint32_t* mask_b,
+                                                             const uint32_t* __restrict__ mask_iter) {
     pdl_enter();
+    if (mask_iter && (*mask_iter & 1u)) mask_cur = mask_b;  // with mask_iter, mask_cur arrives as mask A
     const uint32_t chunks = (n + 31u) >> 5;
     const uint32_t lane = threadIdx.x & 31u;
     const uint32_t stride = gridDim.x * blockDim.x;
@@ -185,16 +187,25 @@ __global__ void __launch_bounds__(256) visible_chunks_kernel(BlockView b, uint32
 // ---------------------------------------------------------------------------------
 // Preprocess (gaussian_point_splatting.cu:17-65 + 147-307)
 // ---------------------------------------------------------------------------------
-// One Gaussian: true if it splats this pass (record and count written).
-template <class Scene>
-__device__ __forceinline__ bool preprocess_one(const PreprocessArgs& a, const Scene& scene, uint32_t gi) {
+__device__ __forceinline__ void splat_samples_biased(u32x2& seed, const SplatRecord& rec, const FrameConst& fc,
+                                                     uint64_t* __restrict__ buffer);
+__device__ __forceinline__ void splat_samples_unbiased(u32x2& seed, const SplatRecord& rec, const FrameConst& fc,
+                                                       uint64_t* __restrict__ buffer);
+
+// One Gaussian: true if it splats this pass (record and count written).  kImmediate: a
+// Gaussian of at most a.immediate_threshold points is splatted here instead, its samples
+// drawn from the seed state the point count left (ENABLE_IMMEDIATE_SPLATTING,
+// gaussian_point_splatting.cu:272-287), and it is no survivor.
+template <class Scene, bool kImmediate>
+__device__ __forceinline__ bool preprocess_one(const PreprocessArgs& a, const Scene& scene, uint32_t gi,
+                                               const uint32_t* __restrict__ mask_prev) {
     const int idx = (int)gi;
     const FrameConst& fc = a.fc;
     bool splats = false;
     do {
         if (idx >= (int)a.n) break;
         if (fc.enable_hier && block_culled(a.blocks, (uint32_t)idx)) break;
-        if (a.only_previously_occluded && mask_bit(a.mask_prev, (uint32_t)idx)) break;
+        if (a.only_previously_occluded && mask_bit(mask_prev, (uint32_t)idx)) break;
         u32x2 seed = make_seed((uint32_t)idx, (uint32_t)a.frame_seed);
         float opacity = scene.opacity((uint32_t)idx);
         if (opacity <= 0.0f) break;
@@ -281,6 +292,16 @@ __device__ __forceinline__ bool preprocess_one(const PreprocessArgs& a, const Sc
         rec.c = make_float4(opacity, color.x, color.y, color.z);
         rec.d = make_uint4((uint32_t)pmin.x | ((uint32_t)pmin.y << 16), (uint32_t)pmax.x | ((uint32_t)pmax.y << 16),
                            (uint32_t)key, (uint32_t)(key >> 32));
+        if constexpr (kImmediate) {
+            if ((int)num_points <= a.immediate_threshold) {
+                for (uint32_t pt = 0; pt < num_points; ++pt) {
+                    if (fc.use_unbiased) splat_samples_unbiased(seed, rec, fc, a.buffer);
+                    else splat_samples_biased(seed, rec, fc, a.buffer);
+                }
+                a.counts[idx] = 0;
+                break;
+            }
+        }
         a.records[idx] = rec;
         a.counts[idx] = num_points;
         splats = true;
@@ -291,9 +312,16 @@ __device__ __forceinline__ bool preprocess_one(const PreprocessArgs& a, const Sc
 // Persistent over 32-Gaussian chunks (one mask word each): a warp takes chunk after chunk, so
 // a pass over a mostly culled scene costs a bit test per Gaussian, not a thread-block launch
 // per 256 Gaussians.
-template <class Scene>
+template <class Scene, bool kImmediate>
 __global__ void __launch_bounds__(256) preprocess_kernel(PreprocessArgs a, Scene scene) {
     pdl_enter();
+    uint32_t* mask_cur = a.mask_cur;
+    const uint32_t* mask_prev = a.mask_prev;
+    if (a.mask_iter) {
+        const bool odd = (*a.mask_iter & 1u) != 0u;
+        mask_cur = odd ? a.mask_pair[1] : a.mask_pair[0];
+        mask_prev = odd ? a.mask_pair[0] : a.mask_pair[1];
+    }
     const uint32_t lane = threadIdx.x & 31u;
     const uint32_t warps = gridDim.x * (blockDim.x >> 5);
     const uint32_t first = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
@@ -301,17 +329,17 @@ __global__ void __launch_bounds__(256) preprocess_kernel(PreprocessArgs a, Scene
         const uint32_t count = *a.chunk_count;
         for (uint32_t i = first; i < count; i += warps) {
             const uint32_t c = __ldg(a.chunk_list + i);
-            const bool splats = preprocess_one(a, scene, (c << 5) + lane);
+            const bool splats = preprocess_one<Scene, kImmediate>(a, scene, (c << 5) + lane, mask_prev);
             const unsigned m = __ballot_sync(0xffffffffu, splats);
-            if (lane == 0) a.mask_cur[c] = m;
+            if (lane == 0) mask_cur[c] = m;
         }
         return;
     }
     const uint32_t chunks = (a.n + 31u) >> 5;
     for (uint32_t c = first; c < chunks; c += warps) {
-        const bool splats = preprocess_one(a, scene, (c << 5) + lane);
+        const bool splats = preprocess_one<Scene, kImmediate>(a, scene, (c << 5) + lane, mask_prev);
         const unsigned m = __ballot_sync(0xffffffffu, splats);
-        if (lane == 0) a.mask_cur[c] = m;
+        if (lane == 0) mask_cur[c] = m;
     }
 }
 
@@ -324,10 +352,11 @@ __global__ void __launch_bounds__(256) preprocess_kernel(PreprocessArgs a, Scene
 // ---------------------------------------------------------------------------------
 
 // One round of a thread's Gaussians (16 consecutive): its mask bits and point counts.
-__device__ __forceinline__ uint32_t scan_load(const ScanArgs& a, uint32_t base, uint32_t cnt[kScanItems]) {
+__device__ __forceinline__ uint32_t scan_load(const ScanArgs& a, const uint32_t* __restrict__ mask, uint32_t base,
+                                              uint32_t cnt[kScanItems]) {
     uint32_t bits = 0;
     if (base < a.n) {
-        bits = (__ldg(&a.mask[base >> 5]) >> (base & 31)) & 0xFFFFu;
+        bits = (__ldg(&mask[base >> 5]) >> (base & 31)) & 0xFFFFu;
         if (a.n - base < (uint32_t)kScanItems) bits &= (1u << (a.n - base)) - 1u;
     }
 #pragma unroll
@@ -383,13 +412,15 @@ __device__ __forceinline__ void block_scan_pair(uint32_t s, uint32_t p, uint32_t
 template <int kScanRounds>
 __global__ void __launch_bounds__(kScanThreads) scan_reduce_kernel(ScanArgs a) {
     pdl_enter();
+    const uint32_t* mask = a.mask;  // (a select, not a runtime index into the parameter array)
+    if (a.mask_iter) mask = (*a.mask_iter & 1u) ? a.mask_pair[1] : a.mask_pair[0];
     const uint32_t tile = blockIdx.x;
     const uint32_t base = tile * (kScanThreads * kScanItems * kScanRounds) + threadIdx.x * (kScanItems * kScanRounds);
     uint32_t surv = 0, pts = 0;
 #pragma unroll
     for (int q = 0; q < kScanRounds; ++q) {
         uint32_t cnt[kScanItems];
-        surv += __popc(scan_load(a, base + q * kScanItems, cnt));
+        surv += __popc(scan_load(a, mask, base + q * kScanItems, cnt));
 #pragma unroll
         for (int i = 0; i < kScanItems; ++i) pts += cnt[i];
     }
@@ -452,13 +483,15 @@ __global__ void __launch_bounds__(kTileScanThreads) scan_tiles_kernel(ScanArgs a
 template <int kScanRounds>
 __global__ void __launch_bounds__(kScanThreads) scan_write_kernel(ScanArgs a) {
     pdl_enter();
+    const uint32_t* mask = a.mask;  // (a select, not a runtime index into the parameter array)
+    if (a.mask_iter) mask = (*a.mask_iter & 1u) ? a.mask_pair[1] : a.mask_pair[0];
     const uint32_t tile = blockIdx.x;
     const uint32_t base = tile * (kScanThreads * kScanItems * kScanRounds) + threadIdx.x * (kScanItems * kScanRounds);
     uint32_t surv = 0, pts = 0;
 #pragma unroll
     for (int q = 0; q < kScanRounds; ++q) {
         uint32_t cnt[kScanItems];
-        surv += __popc(scan_load(a, base + q * kScanItems, cnt));
+        surv += __popc(scan_load(a, mask, base + q * kScanItems, cnt));
 #pragma unroll
         for (int i = 0; i < kScanItems; ++i) pts += cnt[i];
     }
@@ -471,7 +504,7 @@ __global__ void __launch_bounds__(kScanThreads) scan_write_kernel(ScanArgs a) {
     for (int q = 0; q < kScanRounds; ++q) {  // again, now writing (the counts come from L1/L2)
         uint32_t cnt[kScanItems];
         const uint32_t b = base + q * kScanItems;
-        const uint32_t bits = scan_load(a, b, cnt);
+        const uint32_t bits = scan_load(a, mask, b, cnt);
 #pragma unroll
         for (int i = 0; i < kScanItems; ++i) {
             if ((bits >> i) & 1u) {
@@ -492,10 +525,11 @@ __global__ void __launch_bounds__(kScanThreads) scan_write_kernel(ScanArgs a) {
 __global__ void __launch_bounds__(256) tile_owner_kernel(const uint32_t* __restrict__ surv_start,
                                                          uint32_t* __restrict__ tile_first_rank,
                                                          const PassCounters* __restrict__ counters,
-                                                         uint32_t tile_points) {
+                                                         uint32_t tile_points, uint32_t* __restrict__ mask_iter) {
     pdl_enter();
     const uint32_t points = counters->points;
     const uint32_t survivors = counters->survivors;
+    if (mask_iter && points > 0 && blockIdx.x == 0 && threadIdx.x == 0) *mask_iter += 1u;
     if (points == 0 || survivors == 0) return;
     const uint32_t tiles = (uint32_t)(((unsigned long long)points + tile_points - 1) / tile_points);
     for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < tiles; t += gridDim.x * blockDim.x) {
@@ -534,9 +568,9 @@ __device__ __forceinline__ void atomic_add_color(unsigned long long* address, ui
 
 // Biased mode (use_unbiased_2d_splatting = false): samples in the reference's order, each
 // pre-tested and colour-added before the next one is drawn.
-__device__ __forceinline__ void splat_point_biased(uint32_t point, const SplatRecord& rec, const FrameConst& fc,
-                                                   int frame_seed, uint64_t* __restrict__ buffer) {
-    u32x2 seed = make_seed(point, (uint32_t)frame_seed);
+// One point's samples from `seed` onwards (the seed advances, as splatGaussianPoint's does).
+__device__ __forceinline__ void splat_samples_biased(u32x2& seed, const SplatRecord& rec, const FrameConst& fc,
+                                                     uint64_t* __restrict__ buffer) {
     const vec2 pixel_mean = make_v2(rec.a.x, rec.a.y);
     const float c0 = rec.a.z, c1 = rec.a.w, c2 = rec.b.x;
     const vec3 conic = make_v3(rec.b.y, rec.b.z, rec.b.w);
@@ -564,6 +598,12 @@ __device__ __forceinline__ void splat_point_biased(uint32_t point, const SplatRe
         if ((uint64_t)__ldcg(slot) <= view_depth_bits) continue;
         atomic_add_color(slot, key);
     }
+}
+
+__device__ __forceinline__ void splat_point_biased(uint32_t point, const SplatRecord& rec, const FrameConst& fc,
+                                                   int frame_seed, uint64_t* __restrict__ buffer) {
+    u32x2 seed = make_seed(point, (uint32_t)frame_seed);
+    splat_samples_biased(seed, rec, fc, buffer);
 }
 
 // Unbiased mode (the default): the same sample stream, drawn kSplatBatch samples at a time.
@@ -596,9 +636,8 @@ __device__ __forceinline__ void splat_point_biased(uint32_t point, const SplatRe
 #endif
 constexpr int kSplatBatch = GPS_SPLAT_BATCH;
 
-__device__ __forceinline__ void splat_point_unbiased(uint32_t point, const SplatRecord& rec, const FrameConst& fc,
-                                                     int frame_seed, uint64_t* __restrict__ buffer) {
-    u32x2 seed = make_seed(point, (uint32_t)frame_seed);
+__device__ __forceinline__ void splat_samples_unbiased(u32x2& seed, const SplatRecord& rec, const FrameConst& fc,
+                                                       uint64_t* __restrict__ buffer) {
     const vec2 pixel_mean = make_v2(rec.a.x, rec.a.y);
     const float c0 = rec.a.z, c1 = rec.a.w, c2 = rec.b.x;
     const vec3 conic = make_v3(rec.b.y, rec.b.z, rec.b.w);
@@ -666,6 +705,12 @@ __device__ __forceinline__ void splat_point_unbiased(uint32_t point, const Splat
             if ((live >> b) & 1u) atomicMin(reinterpret_cast<unsigned long long*>(buffer) + slot[b], key);
 #endif
     }
+}
+
+__device__ __forceinline__ void splat_point_unbiased(uint32_t point, const SplatRecord& rec, const FrameConst& fc,
+                                                     int frame_seed, uint64_t* __restrict__ buffer) {
+    u32x2 seed = make_seed(point, (uint32_t)frame_seed);
+    splat_samples_unbiased(seed, rec, fc, buffer);
 }
 
 // The same stream with K (points per thread per pass, ss*ss) known at compile time: the K
@@ -1406,20 +1451,21 @@ void launch_block_cull(const BlockView& b, const FrameConst& fc, const HizView& 
     launch_k(block_cull_kernel, (threads + 255) / 256, 256, 0, stream, b, fc, hiz);
 }
 
-void launch_visible_chunks(const BlockView& b, uint32_t n, uint32_t* list, uint32_t* mask_cur, cudaStream_t stream) {
+void launch_visible_chunks(const BlockView& b, uint32_t n, uint32_t* list, uint32_t* mask_a, uint32_t* mask_b,
+                           const uint32_t* mask_iter, cudaStream_t stream) {
     if (n == 0) return;
     const uint32_t chunks = (n + 31u) >> 5;
     const uint32_t want = (chunks + 255u) / 256u;
-    launch_k(visible_chunks_kernel, want < 1184u ? want : 1184u, 256, 0, stream, b, n, list, mask_cur);
+    launch_k(visible_chunks_kernel, want < 1184u ? want : 1184u, 256, 0, stream, b, n, list, mask_a, mask_b, mask_iter);
 }
 
 // Resident blocks of the persistent preprocess on this device, capped by the work.
-template <class Scene>
+template <class Scene, bool kImmediate>
 int preprocess_grid_size(uint32_t n) {
     static int per_sm = 0;
     if (per_sm == 0) {
         int blocks = 0;
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, preprocess_kernel<Scene>, 256, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, preprocess_kernel<Scene, kImmediate>, 256, 0);
         per_sm = blocks < 1 ? 1 : blocks;
     }
     if (g_num_sms == 0) {
@@ -1432,19 +1478,25 @@ int preprocess_grid_size(uint32_t n) {
     return (int)(want < cap ? want : cap);
 }
 
-void launch_preprocess_fp32(const PreprocessArgs& a, const SceneFP32& s, cudaStream_t stream) {
+template <class Scene>
+void launch_preprocess(const PreprocessArgs& a, const Scene& s, cudaStream_t stream) {
     if (a.n == 0) return;
-    launch_k(preprocess_kernel<SceneFP32>, preprocess_grid_size<SceneFP32>(a.n), 256, 0, stream, a, s);
+    if (a.immediate_threshold > 0)
+        launch_k(preprocess_kernel<Scene, true>, preprocess_grid_size<Scene, true>(a.n), 256, 0, stream, a, s);
+    else
+        launch_k(preprocess_kernel<Scene, false>, preprocess_grid_size<Scene, false>(a.n), 256, 0, stream, a, s);
+}
+
+void launch_preprocess_fp32(const PreprocessArgs& a, const SceneFP32& s, cudaStream_t stream) {
+    launch_preprocess(a, s, stream);
 }
 
 void launch_preprocess_half(const PreprocessArgs& a, const SceneHalf& s, cudaStream_t stream) {
-    if (a.n == 0) return;
-    launch_k(preprocess_kernel<SceneHalf>, preprocess_grid_size<SceneHalf>(a.n), 256, 0, stream, a, s);
+    launch_preprocess(a, s, stream);
 }
 
 void launch_preprocess_compressed(const PreprocessArgs& a, const SceneCompressed& s, cudaStream_t stream) {
-    if (a.n == 0) return;
-    launch_k(preprocess_kernel<SceneCompressed>, preprocess_grid_size<SceneCompressed>(a.n), 256, 0, stream, a, s);
+    launch_preprocess(a, s, stream);
 }
 
 static_assert(kScanTile == kScanTileGaussians, "scan tile size");
@@ -1470,7 +1522,8 @@ void launch_scan(const ScanArgs& a, uint32_t scan_tiles, cudaStream_t stream) {
     const uint64_t max_tiles = ((uint64_t)a.max_points + a.tile_points - 1) / a.tile_points;
     const uint64_t want = (max_tiles + 255) / 256;
     const int owner_grid = (int)(want < 1184 ? (want ? want : 1) : 1184);  // 148 SMs x 8
-    launch_k(tile_owner_kernel, owner_grid, 256, 0, stream, a.surv_start, a.tile_first_rank, a.counters, a.tile_points);
+    launch_k(tile_owner_kernel, owner_grid, 256, 0, stream, a.surv_start, a.tile_first_rank, a.counters, a.tile_points,
+             a.mask_iter);
 }
 
 template <int K>

@@ -80,11 +80,23 @@ struct PreprocessArgs {
     BlockView blocks;
     const uint32_t* chunk_list;   // 32-Gaussian chunks with a visible block (null: every chunk)
     const uint32_t* chunk_count;
+    int immediate_threshold;      // > 0: splat Gaussians of <= this many points in the preprocess
+    uint64_t* buffer;             // splat buffer (immediate splatting only)
+    // When mask_iter is set, mask_cur / mask_prev are mask_pair[it & 1] / mask_pair[(it + 1) & 1]
+    // for the device-side pass counter it (see ScanArgs::mask_iter).
+    uint32_t* mask_pair[2];
+    const uint32_t* mask_iter;
 };
 
 struct ScanArgs {
     const uint32_t* counts;
     const uint32_t* mask;
+    // Survivor masks A/B and the device-side pass counter choosing between them (null: `mask`
+    // is used as given).  The counter advances after a pass only when its point total is
+    // non-zero: WorkloadDistributor::build returns before iteration++ when it has no samples
+    // (workload_distributor.cu:107-111,145), so the next pass reuses the same mask pair order.
+    const uint32_t* mask_pair[2];
+    uint32_t* mask_iter;
     uint32_t n;
     uint32_t max_points;
     uint32_t tile_points;        // points per splat tile
@@ -121,7 +133,10 @@ struct ResolveArgs {
 void launch_block_cull(const BlockView& b, const FrameConst& fc, const HizView& hiz, cudaStream_t stream);
 // Lists the 32-Gaussian chunks that hold at least one unculled block and zeroes the survivor
 // mask words of the others.
-void launch_visible_chunks(const BlockView& b, uint32_t n, uint32_t* list, uint32_t* mask_cur, cudaStream_t stream);
+// Zeroes the survivor-mask words of chunks without a visible block in the current mask: mask_a,
+// or the one of (mask_a, mask_b) that *mask_iter selects when mask_iter is set.
+void launch_visible_chunks(const BlockView& b, uint32_t n, uint32_t* list, uint32_t* mask_a, uint32_t* mask_b,
+                           const uint32_t* mask_iter, cudaStream_t stream);
 void launch_preprocess_fp32(const PreprocessArgs& a, const SceneFP32& s, cudaStream_t stream);
 void launch_preprocess_compressed(const PreprocessArgs& a, const SceneCompressed& s, cudaStream_t stream);
 void launch_preprocess_half(const PreprocessArgs& a, const SceneHalf& s, cudaStream_t stream);

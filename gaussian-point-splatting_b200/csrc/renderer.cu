@@ -256,7 +256,7 @@ struct gps_renderer {
     uint64_t cap_mip = 0;         // views of different sizes within these)
     uint32_t cap_n = 0;           // per-Gaussian scratch capacity (a server worker renders any
     uint32_t cap_blocks = 0;      // resident scene up to these sizes)
-    uint32_t iteration = 0;
+    dptr<uint32_t> mask_iter;     // device pass counter selecting the survivor mask pair
     int splat_grid = 0;
     PassCounters* host_counters = nullptr;  // pinned [2]
     cudaEvent_t done = nullptr;
@@ -342,11 +342,11 @@ void render_pass(gps_renderer* r, const FrameConst& fc, int frame, bool first, c
     const int frame_seed = 4 * frame + (first ? 0 : 2);
     BlockView blocks = block_view(r);
     const bool listed = fc.enable_hier && blocks.node_count;
-    uint32_t* mask_cur = r->mask[r->iteration % 2].get();
     if (listed) {
         r->timer.mark(kStCull, st);
         launch_block_cull(blocks, fc, r->hiz, st);
-        launch_visible_chunks(blocks, r->n, r->chunk_list.get(), mask_cur, st);
+        launch_visible_chunks(blocks, r->n, r->chunk_list.get(), r->mask[0].get(), r->mask[1].get(),
+                              r->mask_iter.get(), st);
         count_launch(r, kStCull, 2);
     }
     r->timer.mark(kStPreprocess, st);
@@ -356,13 +356,16 @@ void render_pass(gps_renderer* r, const FrameConst& fc, int frame, bool first, c
     pa.only_previously_occluded = first ? 0 : 1;
     pa.n = r->n;
     pa.counts = r->counts.get();
-    pa.mask_cur = r->mask[r->iteration % 2].get();
-    pa.mask_prev = r->mask[(r->iteration + 1) % 2].get();
+    pa.mask_pair[0] = r->mask[0].get();
+    pa.mask_pair[1] = r->mask[1].get();
+    pa.mask_iter = r->mask_iter.get();
     pa.records = r->records.get();
     pa.hiz = r->hiz;
     pa.blocks = blocks;
     pa.chunk_list = listed ? r->chunk_list.get() : nullptr;
     pa.chunk_count = listed ? r->chunk_count.get() : nullptr;
+    pa.immediate_threshold = r->s.immediate_splat_threshold;
+    pa.buffer = r->buffer.get();
     if (r->scene->format == GPS_SCENE_FP32) {
         SceneFP32 s{r->scene->pos_op.get(), r->scene->rot.get(), r->scene->scale.get(), r->scene->sh.get(), r->n};
         launch_preprocess_fp32(pa, s, st);
@@ -384,7 +387,9 @@ void render_pass(gps_renderer* r, const FrameConst& fc, int frame, bool first, c
     PassCounters* pc = r->counters.get() + (first ? 0 : 1);
     ScanArgs sa{};
     sa.counts = r->counts.get();
-    sa.mask = pa.mask_cur;
+    sa.mask_pair[0] = r->mask[0].get();
+    sa.mask_pair[1] = r->mask[1].get();
+    sa.mask_iter = r->mask_iter.get();
     sa.n = r->n;
     sa.max_points = (uint32_t)std::max(0, r->s.max_number_of_points);
     sa.tile_points = 256;
@@ -408,7 +413,6 @@ void render_pass(gps_renderer* r, const FrameConst& fc, int frame, bool first, c
     sp.n = r->n;
     launch_splat(sp, r->splat_grid, 256, st);
     count_launch(r, kStSplat);
-    r->iteration++;
 }
 
 }  // namespace
@@ -441,6 +445,7 @@ void gps_settings_default(gps_settings* s) {
     s->reduce_point_count = 1;
     s->accumulation_mode = GPS_ACCUM_PROGRESSIVE;
     s->sort_morton_order = 0;
+    s->immediate_splat_threshold = 0;
 }
 
 gps_status gps_settings_parse_args(int32_t argc, const char* const* argv, gps_settings* s, char* model_path,
@@ -702,6 +707,8 @@ gps_status create_renderer(gps_scene* scene, const gps_settings* settings, const
             r->mask[i].reset(dev_alloc<uint32_t>(words + 1));
             GPS_CUDA(cudaMemset(r->mask[i].get(), 0, sizeof(uint32_t) * (words + 1)));
         }
+        r->mask_iter.reset(dev_alloc<uint32_t>(1));
+        GPS_CUDA(cudaMemset(r->mask_iter.get(), 0, sizeof(uint32_t)));
         r->records.reset(dev_alloc<SplatRecord>(std::max<uint32_t>(r->n, 1)));
         r->surv_gid.reset(dev_alloc<uint32_t>(std::max<uint32_t>(r->n, 1)));
         r->surv_start.reset(dev_alloc<uint32_t>(std::max<uint32_t>(r->n, 1)));
@@ -835,7 +842,7 @@ extern "C" {
 gps_status gps_renderer_reset(gps_renderer* r, void* stream) {
     if (!r) return fail(GPS_ERR_INVALID_ARGUMENT, "null argument");
     fill_f32<<<148, 256, 0, as_stream(stream)>>>(r->mip.get(), r->hiz.mip_size, INFINITY);
-    r->iteration = 0;
+    cudaMemsetAsync(r->mask_iter.get(), 0, sizeof(uint32_t), as_stream(stream));
     cudaError_t e = cudaGetLastError();
     return e == cudaSuccess ? GPS_OK : fail(GPS_ERR_CUDA, cudaGetErrorString(e));
 }
@@ -921,9 +928,13 @@ gps_status gps_renderer_debug_view(gps_renderer* r, gps_debug_view* out) {
         if (e != cudaSuccess) return fail(GPS_ERR_CUDA, cudaGetErrorString(e));
     }
     out->counts = r->counts.get();
-    // after a pass the iteration counter has advanced: the last pass wrote mask[(it-1)%2]
-    out->mask_last = r->mask[(r->iteration + 1) % 2].get();
-    out->mask_other = r->mask[r->iteration % 2].get();
+    // the reference's getWeightsMaskPrevious / Current after the frame: mask[(it + 1) % 2] is the
+    // last pass's mask whenever that pass had points (the counter advanced after it)
+    uint32_t it = 0;
+    cudaError_t ce = cudaMemcpy(&it, r->mask_iter.get(), sizeof(uint32_t), cudaMemcpyDeviceToHost);
+    if (ce != cudaSuccess) return fail(GPS_ERR_CUDA, cudaGetErrorString(ce));
+    out->mask_last = r->mask[(it + 1) % 2].get();
+    out->mask_other = r->mask[it % 2].get();
     out->surv_gid = r->surv_gid.get();
     out->surv_start = r->surv_start.get();
     const PassCounters& c = r->host_counters[r->second_pass_last ? 1 : 0];
@@ -990,7 +1001,7 @@ gps_status render_view(gps_renderer* w, const gps_view& v, cudaStream_t st) {
     gps_status rc = configure_view(w, v.width, v.height, v.samples_per_pixel);
     if (rc != GPS_OK) return rc;
     if (w->s.enable_occlusion_culling) fill_f32<<<148, 256, 0, st>>>(w->mip.get(), w->hiz.mip_size, INFINITY);
-    w->iteration = 0;
+    cudaMemsetAsync(w->mask_iter.get(), 0, sizeof(uint32_t), st);
     return render_frame_impl(w, &v.camera, v.d_image, v.d_depth, st);
 }
 

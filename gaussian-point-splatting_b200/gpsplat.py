@@ -68,6 +68,7 @@ class Settings(ctypes.Structure):
         ("background", c_float * 3),
         ("accumulation_mode", c_int32),
         ("sort_morton_order", c_int32),
+        ("immediate_splat_threshold", c_int32),
     ]
 
 

@@ -74,6 +74,11 @@ typedef struct gps_settings {
     float background[3];                        /* 0,0,0 */
     int32_t accumulation_mode;                  /* gps_accumulation, progressive */
     int32_t sort_morton_order;                  /* 0 */
+    /* immediate_splat_threshold: Gaussians of at most this many points are splatted inside
+     * the preprocess (ENABLE_IMMEDIATE_SPLATTING, gaussian_point_splatting.cu:272-287).  The
+     * reference compiles the option out by default, hence 0 = off here; its menu default,
+     * when compiled in, is 8. */
+    int32_t immediate_splat_threshold;          /* 0 */
 } gps_settings;
 
 /* One frame's camera: what RenderSettings carries per frame (render_settings.cuh:94-105). */

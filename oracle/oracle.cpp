@@ -561,8 +561,13 @@ void record_color(const Ctx& c, const FrameC& f, uint32_t idx, Record& r) {
     r.key = (r.key & (0xFFFFFFFull << 36)) | rgb36(col);
 }
 
+void splat_samples(Ctx& c, Seed& seed, const Record& r);
+
 // One preprocess of Gaussian idx; returns the point count (0 = no points) and fills rec.
-uint32_t preprocess_one(const Ctx& c, const FrameC& f, uint32_t idx, int frame_seed, bool only_prev,
+// With immediate_splat_threshold > 0, a Gaussian of at most that many points is splatted here
+// from the seed state the point count left, and counts as no points
+// (ENABLE_IMMEDIATE_SPLATTING, gaussian_point_splatting.cu:272-287, splatGaussianPoint :67-141).
+uint32_t preprocess_one(Ctx& c, const FrameC& f, uint32_t idx, int frame_seed, bool only_prev,
                         const std::vector<uint32_t>& mask_prev, Record& r) {
     const gps_settings& s = c.s;
     Seed seed = make_seed(idx, (uint32_t)frame_seed);
@@ -597,6 +602,10 @@ uint32_t preprocess_one(const Ctx& c, const FrameC& f, uint32_t idx, int frame_s
     uint32_t cap = (uint32_t)(c.up_w * c.up_h / (2 * k));
     n = std::min(n, cap);
     record_color(c, f, idx, r);
+    if (s.immediate_splat_threshold > 0 && (int)n <= s.immediate_splat_threshold) {
+        for (uint32_t pt = 0; pt < n; ++pt) splat_samples(c, seed, r);
+        return 0;
+    }
     return n;
 }
 
@@ -657,9 +666,9 @@ inline void atomic_add_color(uint64_t* p, uint64_t v) {
     }
 }
 
-void splat_point(Ctx& c, uint32_t p, const Record& r, int frame_seed) {
+// One point's samples from `seed` onwards (splatGaussianPoint's inner loop, :98-139).
+void splat_samples(Ctx& c, Seed& seed, const Record& r) {
     const gps_settings& s = c.s;
-    Seed seed = make_seed(p, (uint32_t)frame_seed);
     int k = s.reduce_point_count ? s.supersampling_factor * s.supersampling_factor : 1;
     const int np = s.samples_per_pixel;
     const uint64_t vdb = r.key & (0xFFFFFFFull << 36);
@@ -679,6 +688,11 @@ void splat_point(Ctx& c, uint32_t p, const Record& r, int frame_seed) {
         if (s.use_unbiased_2d_splatting) atomic_min64(slot, r.key);
         else atomic_add_color(slot, r.key);
     }
+}
+
+void splat_point(Ctx& c, uint32_t p, const Record& r, int frame_seed) {
+    Seed seed = make_seed(p, (uint32_t)frame_seed);
+    splat_samples(c, seed, r);
 }
 
 void splat_pass(Ctx& c, int frame_seed, const uint32_t* gid, const uint32_t* start, uint32_t survivors, uint32_t points,
@@ -732,7 +746,9 @@ void render_pass(Ctx& c, const FrameC& f, int frame, bool first, int pass) {
     scan_pass(c);
     c.pts_pass[pass] = c.points;
     splat_pass(c, fs + 1, c.surv_gid.data(), c.surv_start.data(), (uint32_t)c.surv_gid.size(), c.points, c.rec.data());
-    c.iteration++;
+    // WorkloadDistributor::build returns before iteration++ when the pass has no samples
+    // (workload_distributor.cu:107-111,145): the mask pair keeps its order
+    if (c.points > 0) c.iteration++;
 }
 
 }  // namespace

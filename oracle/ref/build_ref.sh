@@ -1,8 +1,9 @@
 #!/usr/bin/env bash
 # Builds the reference's own CUDA frame path (headless) for sm_100a from its sources where
-# they lie, into oracle/_ref/<variant>/ref_harness.  Two variants:
+# they lie, into oracle/_ref/<variant>/ref_harness.  Three variants:
 #   compressed : the reference's default build (config.h defines USE_COMPRESSED_GAUSSIANS)
 #   fp32       : the same sources with a shadow config.h that drops that one define
+#   immediate  : fp32 with the config.h toggle ENABLE_IMMEDIATE_SPLATTING switched on
 # Test infrastructure only: the outputs are checkers, never linked into the library.
 set -euo pipefail
 REF=${GPS_REFERENCE_ROOT:-/root/reference}
@@ -20,6 +21,10 @@ build_variant() {
   mkdir -p "$dir/cfg" "$dir/obj"
   if [ "$variant" = fp32 ]; then
     sed '/^#define USE_COMPRESSED_GAUSSIANS/d' "$REF/src/config.h" > "$dir/cfg/config.h"
+  elif [ "$variant" = immediate ]; then
+    sed -e '/^#define USE_COMPRESSED_GAUSSIANS/d' -e 's|^//#define ENABLE_IMMEDIATE_SPLATTING|#define ENABLE_IMMEDIATE_SPLATTING|' \
+      "$REF/src/config.h" > "$dir/cfg/config.h"
+    grep -q '^#define ENABLE_IMMEDIATE_SPLATTING' "$dir/cfg/config.h"
   else
     cp "$REF/src/config.h" "$dir/cfg/config.h"
   fi
@@ -55,4 +60,4 @@ build_variant() {
   echo "built $dir/ref_harness"
 }
 
-for v in ${GPS_REF_VARIANTS:-compressed fp32}; do build_variant "$v"; done
+for v in ${GPS_REF_VARIANTS:-compressed fp32 immediate}; do build_variant "$v"; done

@@ -128,6 +128,7 @@ static int run_render(int argc, char** argv) {
         else if (a == "--taa") s.accumulationMode = AccumulationMode::TAA;
         else if (a == "--no-accumulation") s.accumulationMode = AccumulationMode::None;
         else if (a == "--sort-morton-order") s.sort_morton_order = true;
+        else if (a == "--immediate-threshold") s.immediate_splat_threshold = atoi(argv[++i]);
         else if (a == "--dump-frames") frames_to_dump = atoi(argv[++i]);
         else if (a == "--checksum-only") dump_full = false;
         else if (a == "--no-post-dump") dump_post = false;

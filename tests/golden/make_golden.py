@@ -11,7 +11,8 @@ sequences, and stores what it produced:
                    offsets, point count and SH colours, plus the camera records and a hash of
                    the PLY bytes the scene was generated as
 
-Usage (on a GPU box, from the repository root):  python tests/golden/make_golden.py
+Usage (on a GPU box, from the repository root):  python tests/golden/make_golden.py [case ...]
+(all fixtures, or only the named cases; GPS_GOLDEN_OUT redirects the output directory)
 """
 from __future__ import annotations
 
@@ -60,7 +61,18 @@ CASES = {
                           dict(width=160, height=90, supersampling_factor=1, samples_per_pixel=1,
                                fully_disable_hierarchical_culling=1, enable_occlusion_culling=0),
                           synth.orbit(1, 30.0, 10.0), "compressed", gpsplat.GPS_SCENE_COMPRESSED),
+    # ENABLE_IMMEDIATE_SPLATTING build: small Gaussians splatted inside the preprocess
+    "immediate_occl_town12k": (lambda: synth.town(12000, seed=9), "town12k_s9",
+                               dict(width=160, height=90, supersampling_factor=2, samples_per_pixel=2,
+                                    immediate_splat_threshold=8),
+                               synth.orbit(2, 30.0, 10.0), "immediate", gpsplat.GPS_SCENE_FP32),
+    "immediate_biased_cube8k": (lambda: synth.cube(8000, seed=21), "cube8k_s21",
+                                dict(width=160, height=90, supersampling_factor=2, samples_per_pixel=1,
+                                     fully_disable_hierarchical_culling=1, enable_occlusion_culling=0,
+                                     use_unbiased_2d_splatting=0, immediate_splat_threshold=4),
+                                [_cube_pose(0)], "immediate", gpsplat.GPS_SCENE_FP32),
 }
+OUT = os.environ.get("GPS_GOLDEN_OUT", HERE)
 
 
 def file_sha256(path):
@@ -117,14 +129,16 @@ def make_case(name):
             out[f"f{i}_culled"] = fr["culled"]
     for k, v in extra.items():
         out[k] = v
-    np.savez_compressed(os.path.join(HERE, f"case_{name}.npz"), **out)
+    np.savez_compressed(os.path.join(OUT, f"case_{name}.npz"), **out)
 
 
 def main():
     if gpsutil.ref_harness("fp32") is None:
         raise SystemExit("reference harness not built: run oracle/ref/build_ref.sh where the reference sources are")
-    make_kat(os.path.join(HERE, "kat.npz"))
-    for name in CASES:
+    names = sys.argv[1:] or list(CASES)
+    if not sys.argv[1:]:
+        make_kat(os.path.join(OUT, "kat.npz"))
+    for name in names:
         make_case(name)
         print("wrote", name, flush=True)
 

@@ -112,6 +112,8 @@ def harness_args(s) -> list[str]:
         a += ["--min-reduce", str(s.occlusion_culling_min_reduce_count)]
     if any(s.background[i] != 0 for i in range(3)):
         a += ["--background"] + [repr(float(s.background[i])) for i in range(3)]
+    if s.immediate_splat_threshold > 0:
+        a += ["--immediate-threshold", str(s.immediate_splat_threshold)]
     if s.accumulation_mode == gpsplat.GPS_ACCUM_TAA:
         a.append("--taa")
     elif s.accumulation_mode == gpsplat.GPS_ACCUM_NONE:

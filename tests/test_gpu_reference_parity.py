@@ -54,6 +54,20 @@ CASES = {
                               supersampling_factor=1, samples_per_pixel=2, fully_disable_hierarchical_culling=1,
                               enable_occlusion_culling=0, use_unbiased_2d_splatting=0, cull_small_gaussians=1),
                               [_cube_cam()], "fp32", gpsplat.GPS_SCENE_FP32),
+    # ENABLE_IMMEDIATE_SPLATTING builds of the reference (menu default threshold 8)
+    "town_immediate_occl": ("town60k", lambda: synth.town(60000, seed=5), dict(width=320, height=180,
+                            supersampling_factor=2, samples_per_pixel=2, immediate_splat_threshold=8),
+                            synth.orbit(3, 30.0, 10.0), "immediate", gpsplat.GPS_SCENE_FP32),
+    # every Gaussian immediate: both passes have zero points, so the reference never advances its
+    # mask pair (pass 2 reads the mask from before the frame)
+    "town_all_immediate": ("town60k", lambda: synth.town(60000, seed=5), dict(width=320, height=180,
+                           supersampling_factor=2, samples_per_pixel=1, immediate_splat_threshold=1000000),
+                           synth.orbit(3, 30.0, 10.0), "immediate", gpsplat.GPS_SCENE_FP32),
+    "cube_immediate_biased_k1": ("cube20k", lambda: synth.cube(20000, seed=11), dict(width=256, height=144,
+                                 supersampling_factor=2, samples_per_pixel=2, reduce_point_count=0,
+                                 use_unbiased_2d_splatting=0, fully_disable_hierarchical_culling=1,
+                                 enable_occlusion_culling=0, immediate_splat_threshold=3), [_cube_cam()],
+                                 "immediate", gpsplat.GPS_SCENE_FP32),
 }
 
 
