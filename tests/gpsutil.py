@@ -211,6 +211,14 @@ def mask_bits(words: np.ndarray, n: int) -> np.ndarray:
     return bits.astype(bool)
 
 
+def written_mask(m: dict, n: int) -> np.ndarray:
+    """The survivor mask the frame's last pass wrote.  The reference advances its mask pair only
+    after a pass with points (workload_distributor.cu:107-111,145), so that is mask_last (its
+    "previous" mask) after a pass with points and mask_other (its "current" one) after an
+    empty pass; its weights array holds the exclusive scan over that mask either way."""
+    return mask_bits(m["mask_last"] if m["points"] > 0 else m["mask_other"], n)
+
+
 def offsets_from(counts: np.ndarray, mask: np.ndarray) -> np.ndarray:
     """Exclusive u32 scan of masked counts (what the reference leaves in its weights array)."""
     c = np.where(mask, counts, 0).astype(np.uint64)

@@ -103,7 +103,7 @@ def test_reference_parity(case):
             mo = _bits(m["mask_other"], n)
             if not np.array_equal(mo_ref, mo):
                 problems.append(f"{tag}: first-pass mask differs at {np.count_nonzero(mo_ref != mo)} Gaussians")
-        offs = gpsutil.offsets_from(m["counts"], ml)
+        offs = gpsutil.offsets_from(m["counts"], gpsutil.written_mask(m, n))
         if not np.array_equal(offs, r["offsets"]):
             problems.append(f"{tag}: point offsets differ at {np.count_nonzero(offs != r['offsets'])} Gaussians")
         st = r["stats"]
