@@ -116,23 +116,7 @@ __device__ __forceinline__ bool aabb_project_bounds(vec3 bmin, vec3 bmax, const 
     return true;
 }
 
-#ifndef GPS_PDL
-#define GPS_PDL 0
-#endif
-// Programmatic dependent launch (GPS_PDL=1): the frame-path kernels are launched with the
-// programmatic stream-serialisation attribute, so a kernel's blocks may be scheduled while the
-// previous kernel of the stream drains.  Each such kernel calls pdl_enter() before its first
-// global-memory access: it waits until the previous kernel has completed and its writes are
-// visible, then allows the next kernel of the stream to begin launching.
-__device__ __forceinline__ void pdl_enter() {
-#if GPS_PDL
-    asm volatile("griddepcontrol.wait;" ::: "memory");
-    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
-#endif
-}
-
 __global__ void __launch_bounds__(256) block_cull_kernel(BlockView b, FrameConst fc, HizView hiz) {
-    pdl_enter();
     const uint32_t idx = blockIdx.x * blockDim.x + threadIdx.x;
     if (idx == 0 && b.chunk_count) *b.chunk_count = 0u;
     const uint32_t word = (idx & ~31u) >> 5;
@@ -161,7 +145,6 @@ __global__ void __launch_bounds__(256) block_cull_kernel(BlockView b, FrameConst
 __global__ void __launch_bounds__(256) visible_chunks_kernel(BlockView b, uint32_t n, uint32_t* __restrict__ list,
                                                              uint32_t* mask_cur, uint32_t* mask_b,
                                                              const uint32_t* __restrict__ mask_iter) {
-    pdl_enter();
     if (mask_iter && (*mask_iter & 1u)) mask_cur = mask_b;  // with mask_iter, mask_cur arrives as mask A
     const uint32_t chunks = (n + 31u) >> 5;
     const uint32_t lane = threadIdx.x & 31u;
@@ -314,7 +297,6 @@ __device__ __forceinline__ bool preprocess_one(const PreprocessArgs& a, const Sc
 // per 256 Gaussians.
 template <class Scene, bool kImmediate>
 __global__ void __launch_bounds__(256) preprocess_kernel(PreprocessArgs a, Scene scene) {
-    pdl_enter();
     uint32_t* mask_cur = a.mask_cur;
     const uint32_t* mask_prev = a.mask_prev;
     if (a.mask_iter) {
@@ -411,7 +393,6 @@ __device__ __forceinline__ void block_scan_pair(uint32_t s, uint32_t p, uint32_t
 // Pass 1 of the scan: every tile's survivor and point totals, fully parallel.
 template <int kScanRounds>
 __global__ void __launch_bounds__(kScanThreads) scan_reduce_kernel(ScanArgs a) {
-    pdl_enter();
     const uint32_t* mask = a.mask;  // (a select, not a runtime index into the parameter array)
     if (a.mask_iter) mask = (*a.mask_iter & 1u) ? a.mask_pair[1] : a.mask_pair[0];
     const uint32_t tile = blockIdx.x;
@@ -436,7 +417,6 @@ __global__ void __launch_bounds__(kScanThreads) scan_reduce_kernel(ScanArgs a) {
 constexpr int kTileScanThreads = 1024;
 constexpr int kTileScanPer = 4;
 __global__ void __launch_bounds__(kTileScanThreads) scan_tiles_kernel(ScanArgs a, uint32_t num_tiles) {
-    pdl_enter();
     __shared__ unsigned long long words[kTileScanThreads * kTileScanPer];
     constexpr uint32_t kRound = kTileScanThreads * kTileScanPer;
     uint32_t carry_s = 0, carry_p = 0;
@@ -482,7 +462,6 @@ __global__ void __launch_bounds__(kTileScanThreads) scan_tiles_kernel(ScanArgs a
 // ids and first points.
 template <int kScanRounds>
 __global__ void __launch_bounds__(kScanThreads) scan_write_kernel(ScanArgs a) {
-    pdl_enter();
     const uint32_t* mask = a.mask;  // (a select, not a runtime index into the parameter array)
     if (a.mask_iter) mask = (*a.mask_iter & 1u) ? a.mask_pair[1] : a.mask_pair[0];
     const uint32_t tile = blockIdx.x;
@@ -526,7 +505,6 @@ __global__ void __launch_bounds__(256) tile_owner_kernel(const uint32_t* __restr
                                                          uint32_t* __restrict__ tile_first_rank,
                                                          const PassCounters* __restrict__ counters,
                                                          uint32_t tile_points, uint32_t* __restrict__ mask_iter) {
-    pdl_enter();
     const uint32_t points = counters->points;
     const uint32_t survivors = counters->survivors;
     if (mask_iter && points > 0 && blockIdx.x == 0 && threadIdx.x == 0) *mask_iter += 1u;
@@ -821,22 +799,10 @@ __device__ __forceinline__ void splat_point_unbiased_k(uint32_t point, const Spl
 #endif
 }
 
-// 1: the tile loop double-buffers its survivor-start table: tile t+1's table loads are issued
-// before tile t's points are splatted (and tile t+2's first rank one tile earlier still), so
-// no dependent global load sits between two tiles; one barrier per tile either way.
-#ifndef GPS_SPLAT_PREFETCH
-#define GPS_SPLAT_PREFETCH 0
-#endif
-
 // K > 0: unbiased splatting with K points per thread per pass; K = 0: any other setting.
 template <int K>
-#if GPS_SPLAT_PREFETCH
-__global__ void __launch_bounds__(kSplatTile, 4) splat_kernel(SplatArgs a) {
-#else
 __global__ void __launch_bounds__(kSplatTile) splat_kernel(SplatArgs a) {
-#endif
-    pdl_enter();
-    __shared__ uint32_t s_start[GPS_SPLAT_PREFETCH ? 2 : 1][kSplatTile];
+    __shared__ uint32_t s_start[kSplatTile];
     __shared__ uint32_t s_spread[kTileSize];
     if (GPS_SPLAT_MORTON_LUT && threadIdx.x < kTileSize) s_spread[threadIdx.x] = morton_spread(threadIdx.x);
     const uint32_t points = a.counters->points;
@@ -872,50 +838,19 @@ __global__ void __launch_bounds__(kSplatTile) splat_kernel(SplatArgs a) {
         const uint32_t r = r0 + threadIdx.x;
         return (r0 < survivors && r < survivors) ? a.surv_start[r] : 0xFFFFFFFFu;
     };
-#if GPS_SPLAT_PREFETCH
-    uint32_t tile = blockIdx.x;
-    if ((unsigned long long)tile * kSplatTile >= points) return;  // uniform over the block
-    uint32_t r0 = a.tile_first_rank[tile];
-    s_start[0][threadIdx.x] = start_of(r0);
-    uint32_t next = tile + gridDim.x;
-    uint32_t next_r0 = (unsigned long long)next * kSplatTile < points ? a.tile_first_rank[next] : 0u;
-    __syncthreads();
-    int buf = 0;
-    for (;;) {
-        const bool has_next = (unsigned long long)next * kSplatTile < points;
-        const uint32_t after = next + gridDim.x;
-        uint32_t next_start = 0xFFFFFFFFu, after_r0 = 0u;
-        if (has_next) {
-            next_start = start_of(next_r0);
-            if ((unsigned long long)after * kSplatTile < points) after_r0 = a.tile_first_rank[after];
-        }
-        splat_tile_point(tile * kSplatTile, r0, s_start[buf]);
-        if (!has_next) break;
-        // s_start[buf ^ 1] was last read before the previous barrier
-        s_start[buf ^ 1][threadIdx.x] = next_start;
-        __syncthreads();
-        buf ^= 1;
-        tile = next;
-        r0 = next_r0;
-        next = after;
-        next_r0 = after_r0;
-    }
-#else
     for (uint32_t tile = blockIdx.x; (unsigned long long)tile * kSplatTile < points; tile += gridDim.x) {
         const uint32_t r0 = a.tile_first_rank[tile];
-        s_start[0][threadIdx.x] = start_of(r0);
+        s_start[threadIdx.x] = start_of(r0);
         __syncthreads();
-        splat_tile_point(tile * kSplatTile, r0, s_start[0]);
+        splat_tile_point(tile * kSplatTile, r0, s_start);
         __syncthreads();
     }
-#endif
 }
 
 // ---------------------------------------------------------------------------------
 // Clear and resolve (gaussian_point_splatting.cu:484-548, 580-585)
 // ---------------------------------------------------------------------------------
 __global__ void clear_kernel(ulonglong2* __restrict__ buf, uint64_t pairs, unsigned long long value) {
-    pdl_enter();
     const ulonglong2 v = make_ulonglong2(value, value);
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < pairs; i += (uint64_t)gridDim.x * blockDim.x)
         buf[i] = v;
@@ -975,7 +910,6 @@ __device__ __forceinline__ void resolve_pixel(const ResolveArgs& a, int x, int y
 // Row-major pixels (any supersampling factor).
 template <bool kDepthOnly>
 __global__ void __launch_bounds__(256) resolve_kernel(ResolveArgs a) {
-    pdl_enter();
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     const int y = blockIdx.y * blockDim.y + threadIdx.y;
     if (x >= a.width || y >= a.height) return;
@@ -997,7 +931,6 @@ __device__ __forceinline__ uint32_t morton_compact(uint32_t a) {
 
 template <bool kDepthOnly>
 __global__ void __launch_bounds__(256) resolve_morton_kernel(ResolveArgs a, int ss_log2) {
-    pdl_enter();
     const uint32_t tile_px = (uint32_t)kTileSize >> ss_log2;
     const uint32_t per_tile_log2 = 2u * (uint32_t)(kTileBits - ss_log2);
     const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1023,7 +956,6 @@ constexpr int kResolveStageBytes = 48 * 1024;
 
 template <bool kDepthOnly>
 __global__ void __launch_bounds__(256) resolve_staged_kernel(ResolveArgs a, int ss_log2, int run_log2) {
-    pdl_enter();
     extern __shared__ uint64_t stage[];
     const uint32_t run = 1u << run_log2;                            // entries per pixel
     const uint32_t g0 = blockIdx.x * blockDim.x;
@@ -1069,7 +1001,6 @@ __device__ __forceinline__ float hiz_op(bool use_min, float a, float b) { return
 
 __global__ void __launch_bounds__(kHizThreads * kHizThreads) hiz_build_kernel(HizView c, const float* __restrict__ src,
                                                                                int min_levels) {
-    pdl_enter();
     __shared__ float sm[kHizThreads * kHizThreads];
     __shared__ int s_last;
     const int L = c.levels - 1;
@@ -1341,7 +1272,6 @@ __global__ void taa_kernel(uint8_t* __restrict__ image, float* __restrict__ out_
                            const float* __restrict__ prev_color, const float* __restrict__ cur_depth,
                            const float* __restrict__ prev_depth, mat4 reproj, float blend, int width, int height,
                            int frame_number) {
-    pdl_enter();
     int idx = blockIdx.x * blockDim.x + threadIdx.x;
     if (idx >= width * height) return;
     int x = idx % width;
@@ -1399,7 +1329,6 @@ __global__ void taa_kernel(uint8_t* __restrict__ image, float* __restrict__ out_
 
 __global__ void progressive_kernel(uint8_t* __restrict__ image, float* __restrict__ cur, float* __restrict__ accum,
                                    int width, int height, int frames) {
-    pdl_enter();
     int idx = blockIdx.x * blockDim.x + threadIdx.x;
     if (idx >= width * height) return;
     vec3 color = ld3(cur, idx);
@@ -1427,21 +1356,7 @@ int g_num_sms = 0;
 namespace {
 template <typename... KArgs, typename... Args>
 void launch_k(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t stream, Args... args) {
-#if GPS_PDL
-    cudaLaunchAttribute attr[1];
-    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-    attr[0].val.programmaticStreamSerializationAllowed = 1;
-    cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = grid;
-    cfg.blockDim = block;
-    cfg.dynamicSmemBytes = smem;
-    cfg.stream = stream;
-    cfg.attrs = attr;
-    cfg.numAttrs = 1;
-    cudaLaunchKernelEx(&cfg, kernel, args...);
-#else
     kernel<<<grid, block, smem, stream>>>(args...);
-#endif
 }
 }  // namespace
 
