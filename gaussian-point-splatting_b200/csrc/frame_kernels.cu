@@ -799,10 +799,19 @@ __device__ __forceinline__ void splat_point_unbiased_k(uint32_t point, const Spl
 #endif
 }
 
+// Points per thread between two block barriers: a block takes kSplatRounds consecutive 256-point
+// tiles at once, with one survivor-start window of kSplatRounds * 256 entries (the survivors
+// owning those points are the first tile's owner and at most that many more).
+#ifndef GPS_SPLAT_ROUNDS
+#define GPS_SPLAT_ROUNDS 1
+#endif
+constexpr int kSplatRounds = GPS_SPLAT_ROUNDS;
+constexpr int kSplatWindow = kSplatTile * kSplatRounds;
+
 // K > 0: unbiased splatting with K points per thread per pass; K = 0: any other setting.
 template <int K>
 __global__ void __launch_bounds__(kSplatTile) splat_kernel(SplatArgs a) {
-    __shared__ uint32_t s_start[kSplatTile];
+    __shared__ uint32_t s_start[kSplatWindow];
     __shared__ uint32_t s_spread[kTileSize];
     if (GPS_SPLAT_MORTON_LUT && threadIdx.x < kTileSize) s_spread[threadIdx.x] = morton_spread(threadIdx.x);
     const uint32_t points = a.counters->points;
@@ -811,7 +820,7 @@ __global__ void __launch_bounds__(kSplatTile) splat_kernel(SplatArgs a) {
     auto splat_tile_point = [&](uint32_t p0, uint32_t r0, const uint32_t* starts) {
         const uint32_t p = p0 + threadIdx.x;
         if (p < points && starts[0] <= p) {
-            int lo = 0, hi = kSplatTile - 1;  // largest k with starts[k] <= p
+            int lo = 0, hi = kSplatWindow - 1;  // largest k with starts[k] <= p
             while (lo < hi) {
                 int mid = (lo + hi + 1) >> 1;
                 if (starts[mid] <= p) lo = mid;
@@ -834,15 +843,17 @@ __global__ void __launch_bounds__(kSplatTile) splat_kernel(SplatArgs a) {
             }
         }
     };
-    auto start_of = [&](uint32_t r0) {
-        const uint32_t r = r0 + threadIdx.x;
+    auto start_of = [&](uint32_t r0, uint32_t k) {
+        const uint32_t r = r0 + k;
         return (r0 < survivors && r < survivors) ? a.surv_start[r] : 0xFFFFFFFFu;
     };
-    for (uint32_t tile = blockIdx.x; (unsigned long long)tile * kSplatTile < points; tile += gridDim.x) {
-        const uint32_t r0 = a.tile_first_rank[tile];
-        s_start[threadIdx.x] = start_of(r0);
+    for (uint32_t group = blockIdx.x; (unsigned long long)group * kSplatWindow < points; group += gridDim.x) {
+        const uint32_t r0 = a.tile_first_rank[group * kSplatRounds];
+#pragma unroll
+        for (int q = 0; q < kSplatRounds; ++q)
+            s_start[q * kSplatTile + threadIdx.x] = start_of(r0, q * kSplatTile + threadIdx.x);
         __syncthreads();
-        splat_tile_point(tile * kSplatTile, r0, s_start);
+        for (int q = 0; q < kSplatRounds; ++q) splat_tile_point(group * kSplatWindow + q * kSplatTile, r0, s_start);
         __syncthreads();
     }
 }
