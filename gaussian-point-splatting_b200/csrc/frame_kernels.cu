@@ -12,6 +12,7 @@
 // Every floating-point expression that decides a sample position, a count or a packed
 // value follows the reference's expression shape (see gps_math.cuh) so that the 64-bit
 // splat buffer is bit-identical to the reference kernels' for the same inputs.
+#include <type_traits>
 #include <cstdio>
 #include <mutex>
 #include <string>
@@ -820,10 +821,10 @@ __global__ void __launch_bounds__(kSplatTile, kSplatRounds > 1 ? 4 : 1) splat_ke
     const uint32_t points = a.counters->points;
     const uint32_t survivors = a.counters->survivors;
     // splats point p0 + threadIdx.x of a tile whose survivor starts are in `starts`
-    auto splat_tile_point = [&](uint32_t p0, uint32_t r0, const uint32_t* starts) {
+    auto splat_tile_point = [&](uint32_t p0, uint32_t r0, const uint32_t* starts, int window) {
         const uint32_t p = p0 + threadIdx.x;
         if (p < points && starts[0] <= p) {
-            int lo = 0, hi = kSplatWindow - 1;  // largest k with starts[k] <= p
+            int lo = 0, hi = window - 1;  // largest k with starts[k] <= p
             while (lo < hi) {
                 int mid = (lo + hi + 1) >> 1;
                 if (starts[mid] <= p) lo = mid;
@@ -850,15 +851,26 @@ __global__ void __launch_bounds__(kSplatTile, kSplatRounds > 1 ? 4 : 1) splat_ke
         const uint32_t r = r0 + k;
         return (r0 < survivors && r < survivors) ? a.surv_start[r] : 0xFFFFFFFFu;
     };
-    for (uint32_t group = blockIdx.x; (unsigned long long)group * kSplatWindow < points; group += gridDim.x) {
-        const uint32_t r0 = a.tile_first_rank[group * kSplatRounds];
+    // grouped tiles only while there are at least two groups per block; a small pass keeps one
+    // tile per barrier so that its points still spread over every block
+    auto walk = [&](auto rounds_c) {
+        constexpr uint32_t rounds = decltype(rounds_c)::value;
+        constexpr uint32_t group_points = kSplatTile * rounds;
+        for (uint32_t group = blockIdx.x; (unsigned long long)group * group_points < points; group += gridDim.x) {
+            const uint32_t r0 = a.tile_first_rank[group * rounds];
 #pragma unroll
-        for (int q = 0; q < kSplatRounds; ++q)
-            s_start[q * kSplatTile + threadIdx.x] = start_of(r0, q * kSplatTile + threadIdx.x);
-        __syncthreads();
-        for (int q = 0; q < kSplatRounds; ++q) splat_tile_point(group * kSplatWindow + q * kSplatTile, r0, s_start);
-        __syncthreads();
-    }
+            for (uint32_t q = 0; q < rounds; ++q)
+                s_start[q * kSplatTile + threadIdx.x] = start_of(r0, q * kSplatTile + threadIdx.x);
+            __syncthreads();
+            for (uint32_t q = 0; q < rounds; ++q)
+                splat_tile_point(group * group_points + q * kSplatTile, r0, s_start, (int)group_points);
+            __syncthreads();
+        }
+    };
+    if ((unsigned long long)points >= 2ull * gridDim.x * kSplatWindow)
+        walk(std::integral_constant<uint32_t, (uint32_t)kSplatRounds>{});
+    else
+        walk(std::integral_constant<uint32_t, 1u>{});
 }
 
 // ---------------------------------------------------------------------------------
