@@ -57,19 +57,32 @@ def workload_spec(name: str):
 
 def load_scene_host(spec) -> np.ndarray:
     """Activated CPUGaussian array (N x 59 float32), cached on local disk per box."""
+    return load_scene_files(spec)[1]
+
+
+def load_scene_files(spec):
+    """(PLY path, activated host array) of the workload's scene, generated once per box.  The
+    PLY (3DGS binary layout, with the bvh_sorted_order comment) is what the library's
+    gps_scene_load_ply and the reference's own loader read; the activated array feeds the CPU
+    baseline."""
     os.makedirs(SCENE_CACHE, exist_ok=True)
-    path = os.path.join(SCENE_CACHE, f"{spec['kind']}{spec['n']}_act.npy")
-    if os.path.exists(path):
-        return np.load(path, mmap_mode="r")
+    stem = os.path.join(SCENE_CACHE, f"{spec['kind']}{spec['n']}")
+    ply, act = stem + ".ply", stem + "_act.npy"
+    if os.path.exists(ply) and os.path.exists(act):
+        return ply, np.load(act, mmap_mode="r")
     t = time.time()
     raw = synth.town(spec["n"]) if spec["kind"] == "town" else synth.cube(spec["n"])
+    if not os.path.exists(ply):
+        tmp = ply + f".{os.getpid()}.tmp"
+        raw.write_ply(tmp)
+        os.replace(tmp, ply)
     g = synth.activate(raw)
     del raw
     log(f"generated {spec['kind']} scene with {spec['n']} Gaussians in {time.time() - t:.1f}s")
-    tmp = path + f".{os.getpid()}.tmp.npy"
+    tmp = act + f".{os.getpid()}.tmp.npy"
     np.save(tmp, g)
-    os.replace(tmp, path)
-    return g
+    os.replace(tmp, act)
+    return ply, g
 
 
 def poses_for(spec):
@@ -189,22 +202,32 @@ def barrier(world: int):
 # ---------------------------------------------------------------------------------
 # CPU baseline (the oracle, oracle/oracle.cpp) on a bounded sample of the workload
 # ---------------------------------------------------------------------------------
-def stage_rooflines(stages, spec, n, entries, surv, passes, w, h, peak):
+# bytes the preprocess reads per Gaussian it loads (opacity + geometry) and per survivor (SH),
+# by scene format: FP32 SoA (16 B position+opacity, 16 B rotation, 16 B scale; 192 B SH),
+# the reference's compressed format (16 B quantised geometry + 1 B opacity; 64 B compact SH),
+# and the half format (16 B + 16 B records; 48 B FP8 AC coefficients)
+PREPROCESS_BYTES = {"fp32": (48.0, 192.0), "compressed": (17.0, 64.0), "half": (32.0, 48.0)}
+
+
+def stage_rooflines(stages, spec, st, entries, passes, w, h, peak):
     """Achieved algorithmic GB/s of the HBM-bound stages, per launch, against the measured copy
-    peak.  Algorithmic bytes per launch (survivors from the device counters, FP32 scene):
-      preprocess  n/8 mask + 48 per Gaussian (position, rotation, scale) + per survivor 192 SH
-                  + 64 record + 4 count; reported without block culling only (every Gaussian
-                  is then tested)
-      scan        n/8 mask, read twice, + 4 per survivor count read twice + 8 per survivor written
+    peak.  Algorithmic bytes per launch (counts from the device counters of the last frame):
+      preprocess  per Gaussian whose attributes were read (device tally, after the block cull
+                  and pass 2's previous-mask test): its geometry; per survivor: its SH, the
+                  64-byte splat record and the 4-byte count; per 32 Gaussians read: the mask
+                  word read and written
+      scan        per 32 Gaussians: the mask word, read twice; per survivor: its count read
+                  twice and 8 bytes of workload written
       resolve     8 per splat-buffer entry + 16 per pixel (final) / 4 (depth-only), averaged
       clear       8 per splat-buffer entry"""
     out = {}
-    s_pass = surv / max(1, passes)
+    n = spec["n"] * spec.get("tiles", 1) ** 2
+    read = (st.gaussians_read_one + st.gaussians_read_two) / max(1, passes)
+    surv = (st.survivors_one + st.survivors_two) / max(1, passes)
+    geom, sh = PREPROCESS_BYTES[spec.get("fmt", "fp32")]
     model = {
-        # without block culling every Gaussian is tested; with it the tested count is unknown here
-        "preprocess": (n / 8.0 + n * 48.0 + s_pass * (192.0 + 64.0 + 4.0))
-        if spec.get("fmt") != "half" and not spec.get("hier") else None,
-        "scan": n / 4.0 + s_pass * (8.0 + 8.0),
+        "preprocess": read * geom + surv * (sh + 64.0 + 4.0) + read / 32.0 * 8.0 if read > 0 else None,
+        "scan": n / 4.0 + surv * (8.0 + 8.0),
         "resolve": 8.0 * entries + (10.0 if passes == 2 else 16.0) * w * h,
         "clear": 8.0 * entries,
     }
@@ -217,69 +240,99 @@ def stage_rooflines(stages, spec, n, entries, surv, passes, w, h, peak):
         per = ms / launches
         gbs = b / (per / 1000.0) / 1e9
         out[k] = {"achieved_gbs": gbs, "frac": gbs / peak, "ms_per_launch": per, "algorithmic_bytes": b}
+        if k == "preprocess":
+            out[k]["gaussians_read_per_pass"] = read
+            out[k]["survivors_per_pass"] = surv
     return out
 
 
-def measured_traffic(kernel: str, spec):
-    """DRAM bytes per splat launch from the committed ncu summary (dram__bytes_read.sum +
-    dram__bytes_write.sum, averaged over a frame's two launches).  The splat's traffic follows
-    its buffer (1080p, ss 2, 4 spp for every town workload), not the Gaussian count."""
-    if kernel != "splat" or spec.get("kind") != "town" or (spec["width"], spec["height"], spec["ss"], spec["spp"]) != (1920, 1080, 2, 4):
-        return None
+def measured_traffic(kernel: str, spec, workload: str):
+    """DRAM bytes per launch of the dominant kernel (dram__bytes_read.sum +
+    dram__bytes_write.sum) from the committed ncu summary of the same workload, averaged over a
+    frame's launches; None when no capture of this workload is committed."""
+    path = os.path.join(ROOT, "profiles", f"{kernel}_traffic_{workload}.md")
     try:
-        with open(os.path.join(ROOT, "profiles", "kernels_town4m_1080p_ss2_spp4_full.md")) as f:
+        with open(path) as f:
             for ln in f:
                 if ln.startswith("traffic_per_launch_bytes:"):
-                    return float(ln.split(":")[1])
+                    return float(ln.split(":")[1]), os.path.relpath(path, ROOT)
     except OSError:
         pass
-    return None
+    return None, None
 
 
-def cpu_baseline(gpsplat, g_host, spec, settings, poses, budget_s: float = 12.0):
+def host_cameras(spec, settings, poses, count, phase=0):
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle
 
-    cores = os.cpu_count() or 1
-    n_total = g_host.shape[0]
-    sample_n = min(n_total, 1_000_000)
-    sub = np.ascontiguousarray(g_host[:sample_n])
-    o = oracle.Oracle(sub, settings, threads=cores)
-    cams = make_cameras(gpsplat, settings, poses, max(1, len(poses)), 0)
+    return [oracle.camera_host(*poses[(phase + i) % len(poses)], settings, i + 1) for i in range(count)]
+
+
+def host_settings(spec):
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+
+    return oracle.settings_host(
+        width=spec["width"], height=spec["height"], supersampling_factor=spec["ss"], samples_per_pixel=spec["spp"],
+        reduce_point_count=spec["reduce"], enable_hierarchical_culling=spec["hier"],
+        fully_disable_hierarchical_culling=0 if spec["hier"] else 1, enable_occlusion_culling=spec["occl"],
+        accumulation_mode=1 if spec["taa"] else 2)
+
+
+def cpu_frames(g_host, spec, frames: int, threads: int, budget_s: float = 1e9):
+    """Full frames of the workload (the whole scene, its camera path from the first keyframe)
+    rendered by the CPU oracle with `threads` host threads; returns (frames done, seconds)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+
+    s = host_settings(spec)
+    cams = host_cameras(spec, s, poses_for(spec), frames)
+    o = oracle.Oracle(np.ascontiguousarray(g_host), s, threads=threads)
     t0 = time.time()
-    frames = 0
-    while True:
-        o.render(cams[frames % len(cams)])
-        frames += 1
-        if time.time() - t0 > budget_s or frames >= 64:
+    done = 0
+    for c in cams:
+        o.render(c)
+        done += 1
+        if time.time() - t0 > budget_s:
             break
     dt = time.time() - t0
     o.close()
-    return {"value": sample_n * frames / dt, "unit": "Gaussians/s", "cores": cores, "kind": "port",
-            "sample": f"first {sample_n} of {n_total} Gaussians (Morton-ordered contiguous block), {frames} frames "
-                      f"of the same camera path and settings, {dt:.1f}s"}
+    return done, dt
+
+
+def cpu_baseline(g_host, spec, frames_all: int = 2, frames_one: int = 1):
+    """The CPU restatement of the estimator (oracle/) on the whole scene: `frames_all` frames on
+    every host core, then `frames_one` frame(s) on one core."""
+    cores = os.cpu_count() or 1
+    n = g_host.shape[0]
+    f_all, dt_all = cpu_frames(g_host, spec, frames_all, cores)
+    out = {"value": n * f_all / dt_all, "unit": "Gaussians/s", "cores": cores, "kind": "port",
+           "sample": f"the whole {n}-Gaussian scene, {f_all} frames of its camera path from the first keyframe, "
+                     f"{dt_all:.1f}s on {cores} threads"}
+    if frames_one > 0:
+        f_one, dt_one = cpu_frames(g_host, spec, frames_one, 1)
+        out["one_thread"] = {"value": n * f_one / dt_one, "unit": "Gaussians/s", "cores": 1,
+                             "sample": f"the whole scene, {f_one} frame(s), {dt_one:.1f}s"}
+    return out
 
 
 def run_reference_arm(args, spec, world, rank):
+    """The reference has no CPU implementation of this path; its CPU restatement (oracle/) is
+    timed on every host core, whole frames of the same scene and camera path: one warm-up frame,
+    then up to `steps` frames within a bounded time.  Nothing here loads the CUDA library."""
     if rank != 0:
         return 0
-    import gpsplat
-
-    gpsplat.load_library()
     g = load_scene_host(spec)
-    s = settings_for(gpsplat, spec)
-    poses = poses_for(spec)
-    per_step = []
-    cb = None
-    for k in range(args.warmup + args.steps):
-        cb = cpu_baseline(gpsplat, g, spec, s, poses, budget_s=max(2.0, 20.0 / max(1, args.steps)))
-        if k >= args.warmup:
-            per_step.append(cb["value"])
-    value = float(np.mean(per_step))
-    cb["value"] = value
+    cores = os.cpu_count() or 1
+    warm, _ = cpu_frames(g, spec, args.warmup, cores, budget_s=30.0)  # page the scene in
+    done, dt = cpu_frames(g, spec, args.steps, cores, budget_s=REFERENCE_ARM_BUDGET_S)
+    value = spec["n"] * done / dt
+    cb = {"value": value, "unit": "Gaussians/s", "cores": cores, "kind": "port",
+          "sample": f"the whole {spec['n']}-Gaussian scene, {done} of {args.steps} frames of its camera path "
+                    f"({dt:.1f}s; frames stop after {REFERENCE_ARM_BUDGET_S:.0f}s), {warm} warm-up frame(s)"}
     line = {"impl": "reference", "metric": "Gaussians/sec", "value": value, "unit": "Gaussians/s", "n_gpus": world,
-            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded town, see synth.py)",
+            "steps": done, "warmup": warm, "ms_per_step": 1000.0 * dt / max(1, done), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": f"synthetic (seeded {spec['kind']}, see synth.py)",
             "config": {"workload": args.workload, "gaussians": spec["n"], "resolution": [spec["width"], spec["height"]],
                        "supersampling": spec["ss"], "spp": spec["spp"], "culling": bool(spec["hier"]),
                        "taa": bool(spec["taa"])},
@@ -287,6 +340,66 @@ def run_reference_arm(args, spec, world, rank):
             "e2e": {"value": value, "unit": "Gaussians/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
+
+
+REFERENCE_ARM_BUDGET_S = 150.0
+
+
+def reference_cuda(gpsplat, ply, spec, settings, cams, warmup, mine_ms):
+    """Frame time of the reference's own CUDA kernels on this GPU, same PLY, cameras and
+    settings: the headless build of the reference's sources (oracle/ref/build_ref.sh; its
+    GaussianPointSplatting::render plus the RenderServer post-process, timed per frame with CUDA
+    events, its per-pass host synchronisations included), in its FP32 and its default
+    compressed format.  `mine_ms` maps each format to this library's ms/frame on the same frames."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import tempfile
+
+    import gpsutil
+
+    out = {}
+    work = tempfile.mkdtemp(prefix="gps_refcuda_")
+    camf = os.path.join(work, "cams.bin")
+    gpsutil.write_camera_file(camf, cams)
+    for variant in ("fp32", "compressed"):
+        exe = gpsutil.ref_harness(variant)
+        if exe is None:
+            out[variant] = {"unavailable": "reference build missing (oracle/ref/build_ref.sh)"}
+            continue
+        args = [exe, "render", ply, work, camf] + gpsutil.harness_args(settings, taa_race_free=False) + \
+            ["--checksum-only", "--time", "--warmup", str(warmup), "--dump-frames", "0", "--no-post-dump"]
+        t = time.time()
+        res = subprocess.run(args, capture_output=True, text=True, timeout=1800)
+        if res.returncode != 0:
+            out[variant] = {"unavailable": f"reference harness failed ({res.returncode}): {res.stderr[-300:]}"}
+            continue
+        ref = json.loads([ln for ln in res.stdout.splitlines() if ln.startswith("{")][-1])
+        entry = {"reference_ms_per_frame": ref["ms_per_frame"], "frames": ref["frames"], "wall_s": time.time() - t}
+        if mine_ms.get(variant):
+            entry["ms_per_frame"] = mine_ms[variant]
+            entry["speedup"] = ref["ms_per_frame"] / mine_ms[variant]
+        out[variant] = entry
+    return out
+
+
+def time_frames(gpsplat, scene, settings, cams, warmup, stream):
+    """Device ms per frame of the frame loop over `cams` after `warmup` of them."""
+    import torch
+
+    r = gpsplat.Renderer(scene, settings)
+    loop = gpsplat.FrameLoop(r)
+    for c in cams[:warmup]:
+        loop.step(c, stream.cuda_stream)
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for c in cams[warmup:]:
+        loop.step(c, stream.cuda_stream)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    loop.close()
+    r.close()
+    return e0.elapsed_time(e1) / max(1, len(cams) - warmup)
 
 
 # ---------------------------------------------------------------------------------
@@ -506,6 +619,8 @@ def main():
     ap.add_argument("--impl", default="mine", choices=["mine", "reference"])
     ap.add_argument("--workload", default="town16m", choices=["town16m", "town4m", "town256m", "cube1m", "batch64", "serve"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-reference-cuda", action="store_true", help="skip timing the reference's CUDA build")
+    ap.add_argument("--quick-cpu", action="store_true", help="CPU baseline on all cores only (no 1-thread frame)")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     world, rank, local = dist_init()
@@ -533,7 +648,7 @@ def main():
     import gpsplat
 
     gpsplat.load_library()
-    g_host = load_scene_host(spec)
+    ply, g_host = load_scene_files(spec)
     t = time.time()
     if spec.get("fmt") == "half":
         base_scene = gpsplat.Scene.from_host(np.ascontiguousarray(g_host), gpsplat.GPS_SCENE_HALF, presorted=True)
@@ -542,7 +657,8 @@ def main():
         scene = base_scene.tile([[(i - (k - 1) / 2) * ext, (j - (k - 1) / 2) * ext] for j in range(k) for i in range(k)])
         base_scene.close()
     else:
-        scene = gpsplat.Scene.from_host(np.ascontiguousarray(g_host), presorted=True)
+        # through the reference-facing loader (gps_scene_load_ply), as a drop-in user loads it
+        scene = gpsplat.Scene.from_ply(ply, gpsplat.GPS_SCENE_FP32)
     log(f"rank {rank}: scene uploaded in {time.time() - t:.1f}s")
     s = settings_for(gpsplat, spec)
     r = gpsplat.Renderer(scene, s)
@@ -560,7 +676,7 @@ def main():
     torch.cuda.synchronize()
     r.enable_timing(False)
 
-    # ---- device-timed region: K frames, inputs resident (scene > L2 every frame) ----
+    # ---- device-timed region: K frames, inputs resident (splat buffer 2x L2 every frame) ----
     sampler = ClockSampler(local)
     barrier(world)
     torch.cuda.synchronize()
@@ -626,7 +742,6 @@ def main():
     dom = max(stages, key=lambda k: stages[k][0])
     dom_ms, dom_launches = stages[dom]
     per_launch_ms = dom_ms / max(1, dom_launches)
-    ntot = n_scene
     entries = r.splat_buffer()[1]
     surv = st.survivors_one + st.survivors_two
     passes = 2 if spec["occl"] else 1
@@ -634,48 +749,63 @@ def main():
         # compulsory traffic of a splat launch: each survivor's 64-byte record and 8 bytes of
         # workload, one read and one write of every splat-buffer entry
         alg_bytes = (72.0 * surv / passes) + 16.0 * entries
-    elif dom == "preprocess":
-        alg_bytes = ntot * 48.0 + (surv / passes) * (192.0 + 64.0 + 4.0) + ntot / 8.0
     elif dom == "resolve":
         alg_bytes = 8.0 * entries + 16.0 * w * h
     else:
-        alg_bytes = 8.0 * entries
+        alg_bytes = stage_rooflines(stages, spec, st, entries, passes, w, h, hbm_peak).get(dom, {}).get(
+            "algorithmic_bytes", 8.0 * entries)
     achieved = alg_bytes / (per_launch_ms / 1000.0) / 1e9
-    traffic = measured_traffic(dom, spec)
+    traffic, traffic_src = measured_traffic(dom, spec, args.workload)
     roofline = {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
                 "frac": achieved / hbm_peak, "traffic": traffic, "peak_source": peak_src,
                 "algorithmic_bytes_per_launch": alg_bytes, "ms_per_launch": per_launch_ms,
-                "traffic_source": "profiles/kernels_town4m_1080p_ss2_spp4_full.md (ncu dram bytes of the same "
-                                  "1080p ss 2, 4 spp splat buffer)" if traffic else None}
+                "traffic_source": traffic_src}
 
+    l2_note = (f"inputs larger than L2: the {8 * entries / 1e6:.0f} MB splat buffer is cleared, scattered into and "
+               f"resolved every frame; the preprocess reads the attributes of the Gaussians that pass the block cull "
+               f"({(st.gaussians_read_one + st.gaussians_read_two) / passes / 1e6:.1f}M per pass)")
     line = {
         "metric": "Gaussians/sec", "value": value, "unit": "Gaussians/s", "n_gpus": world, "steps": K,
         "warmup": args.warmup, "ms_per_step": dev_ms_max / K, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded town, see synth.py)",
+        "vs_baseline": None, "dtype": "f32", "data": f"synthetic (seeded {spec['kind']}, see synth.py)",
         "config": {"workload": args.workload, "gaussians": n_scene, "resolution": [w, h], "supersampling": spec["ss"],
                    "spp": spec["spp"], "points_per_thread": spec["ss"] ** 2 if spec["reduce"] else 1,
                    "culling": bool(spec["hier"]), "occlusion": bool(spec["occl"]), "taa": bool(spec["taa"]),
                    "camera_path": f"{len(poses)}-frame orbit r=30 h=10" if spec["kind"] == "town" else "static",
-                   "l2": "inputs larger than L2 (scene >= 3.8 GB read every frame)", "parallelism": f"replicas x{world}"},
+                   "l2": l2_note, "parallelism": f"replicas x{world}"},
         "clocks": clocks,
         "e2e": {"value": e2e_value, "unit": "Gaussians/s", "h2d_bytes_per_step": cam_bytes,
                 "d2h_bytes_per_step": h * w * 3, "ms_per_step": e2e_ms / K, "wall_s": wall_e2e},
         "gpu_launches": int(launches_per_frame * K),
         "roofline": roofline,
         "stages_ms_per_frame": {k: v[0] / K for k, v in stages.items()},
-        "stage_rooflines": stage_rooflines(stages, spec, n_scene, entries, surv, passes, w, h, hbm_peak),
+        "stage_rooflines": stage_rooflines(stages, spec, st, entries, passes, w, h, hbm_peak),
         "points_per_frame": [st.num_points_one, st.num_points_two],
         "survivors_per_frame": [st.survivors_one, st.survivors_two],
+        "gaussians_read_per_frame": [st.gaussians_read_one, st.gaussians_read_two],
     }
     if spec.get("fmt") == "half":
         line["dtype"] = "f16/fp8 storage, f32 arithmetic"
         line["config"]["format"] = "half (GPS_SCENE_HALF), town tiled %dx%d" % (spec["tiles"], spec["tiles"])
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline(gpsplat, g_host, spec, s, poses)
-    if rank == 0:
-        print(json.dumps(line), flush=True)
     loop.close()
     r.close()
+    if rank == 0 and world == 1 and spec.get("fmt") != "half" and not args.no_reference_cuda:
+        # the reference's own CUDA kernels on the same PLY, cameras and settings, beside this
+        # library's frame loop on the same frames in the same two formats
+        mine = {"fp32": time_frames(gpsplat, scene, s, cams, args.warmup, stream)}
+        comp = gpsplat.Scene.from_ply(ply, gpsplat.GPS_SCENE_COMPRESSED)
+        mine["compressed"] = time_frames(gpsplat, comp, s, cams, args.warmup, stream)
+        comp.close()
+        line["reference_cuda"] = reference_cuda(gpsplat, ply, spec, s, cams, args.warmup, mine)
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        if spec.get("fmt") == "half":
+            line["cpu_baseline"] = {"value": None, "unit": "Gaussians/s", "cores": os.cpu_count() or 1, "kind": "port",
+                                    "sample": "none: the CPU restatement has no half-precision format and the tiled "
+                                              "256M scene does not fit its host-memory layout"}
+        else:
+            line["cpu_baseline"] = cpu_baseline(g_host, spec, frames_all=2, frames_one=0 if args.quick_cpu else 1)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
     scene.close()
     if world > 1:
         import torch.distributed as dist

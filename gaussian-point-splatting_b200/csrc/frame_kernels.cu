@@ -182,14 +182,16 @@ __device__ __forceinline__ void splat_samples_unbiased(u32x2& seed, const SplatR
 // gaussian_point_splatting.cu:272-287), and it is no survivor.
 template <class Scene, bool kImmediate>
 __device__ __forceinline__ bool preprocess_one(const PreprocessArgs& a, const Scene& scene, uint32_t gi,
-                                               const uint32_t* __restrict__ mask_prev) {
+                                               const uint32_t* __restrict__ mask_prev, bool& loaded) {
     const int idx = (int)gi;
     const FrameConst& fc = a.fc;
     bool splats = false;
+    loaded = false;
     do {
         if (idx >= (int)a.n) break;
         if (fc.enable_hier && block_culled(a.blocks, (uint32_t)idx)) break;
         if (a.only_previously_occluded && mask_bit(mask_prev, (uint32_t)idx)) break;
+        loaded = true;
         u32x2 seed = make_seed((uint32_t)idx, (uint32_t)a.frame_seed);
         float opacity = scene.opacity((uint32_t)idx);
         if (opacity <= 0.0f) break;
@@ -308,22 +310,22 @@ __global__ void __launch_bounds__(256) preprocess_kernel(PreprocessArgs a, Scene
     const uint32_t lane = threadIdx.x & 31u;
     const uint32_t warps = gridDim.x * (blockDim.x >> 5);
     const uint32_t first = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    uint32_t loaded_tally = 0;  // this warp's Gaussians whose attributes were read
+    auto chunk = [&](uint32_t c) {
+        bool loaded;
+        const bool splats = preprocess_one<Scene, kImmediate>(a, scene, (c << 5) + lane, mask_prev, loaded);
+        const unsigned m = __ballot_sync(0xffffffffu, splats);
+        loaded_tally += (uint32_t)__popc(__ballot_sync(0xffffffffu, loaded));
+        if (lane == 0) mask_cur[c] = m;
+    };
     if (a.chunk_list) {
         const uint32_t count = *a.chunk_count;
-        for (uint32_t i = first; i < count; i += warps) {
-            const uint32_t c = __ldg(a.chunk_list + i);
-            const bool splats = preprocess_one<Scene, kImmediate>(a, scene, (c << 5) + lane, mask_prev);
-            const unsigned m = __ballot_sync(0xffffffffu, splats);
-            if (lane == 0) mask_cur[c] = m;
-        }
-        return;
+        for (uint32_t i = first; i < count; i += warps) chunk(__ldg(a.chunk_list + i));
+    } else {
+        const uint32_t chunks = (a.n + 31u) >> 5;
+        for (uint32_t c = first; c < chunks; c += warps) chunk(c);
     }
-    const uint32_t chunks = (a.n + 31u) >> 5;
-    for (uint32_t c = first; c < chunks; c += warps) {
-        const bool splats = preprocess_one<Scene, kImmediate>(a, scene, (c << 5) + lane, mask_prev);
-        const unsigned m = __ballot_sync(0xffffffffu, splats);
-        if (lane == 0) mask_cur[c] = m;
-    }
+    if (a.loaded && lane == 0 && loaded_tally) atomicAdd(a.loaded, loaded_tally);
 }
 
 // ---------------------------------------------------------------------------------
@@ -455,7 +457,9 @@ __global__ void __launch_bounds__(kTileScanThreads) scan_tiles_kernel(ScanArgs a
         a.counters->points = carry_p < a.max_points ? carry_p : a.max_points;
         a.counters->truncated = carry_p > a.max_points ? 1u : 0u;
         a.counters->scan_timeouts = 0u;
-        a.counters->pad[0] = a.counters->pad[1] = a.counters->pad[2] = 0u;
+        a.counters->loaded = a.loaded ? *a.loaded : 0u;
+        if (a.loaded) *a.loaded = 0u;  // the next pass's preprocess tallies from zero
+        a.counters->pad[0] = a.counters->pad[1] = 0u;
     }
 }
 
@@ -502,13 +506,18 @@ __global__ void __launch_bounds__(kScanThreads) scan_write_kernel(ScanArgs a) {
 // a binary search over the survivors' first points (monotone below 2^32 points per pass).  A
 // survivor can own thousands of tiles (a Gaussian right in front of the camera), so this is
 // done per tile rather than per survivor.
+// With `bins` set the survivors are in screen-bin order: their count is the binned one
+// (counters->pad[0]) and the bin cursors are cleared here for the next pass.
 __global__ void __launch_bounds__(256) tile_owner_kernel(const uint32_t* __restrict__ surv_start,
                                                          uint32_t* __restrict__ tile_first_rank,
                                                          const PassCounters* __restrict__ counters,
-                                                         uint32_t tile_points, uint32_t* __restrict__ mask_iter) {
+                                                         uint32_t tile_points, uint32_t* __restrict__ mask_iter,
+                                                         unsigned long long* __restrict__ bins, uint32_t nbins) {
     const uint32_t points = counters->points;
-    const uint32_t survivors = counters->survivors;
+    const uint32_t survivors = bins ? counters->pad[0] : counters->survivors;
     if (mask_iter && points > 0 && blockIdx.x == 0 && threadIdx.x == 0) *mask_iter += 1u;
+    if (bins)
+        for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i <= nbins; i += gridDim.x * blockDim.x) bins[i] = 0ull;
     if (points == 0 || survivors == 0) return;
     const uint32_t tiles = (uint32_t)(((unsigned long long)points + tile_points - 1) / tile_points);
     for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < tiles; t += gridDim.x * blockDim.x) {
@@ -520,6 +529,87 @@ __global__ void __launch_bounds__(256) tile_owner_kernel(const uint32_t* __restr
             else hi = mid - 1;
         }
         tile_first_rank[t] = lo;
+    }
+}
+
+// ---------------------------------------------------------------------------------
+// Screen-tile binning of a pass's survivors (BinArgs): a histogram of (survivors, points) per
+// bin, an in-place exclusive scan of the bins, then a scatter in which each survivor takes its
+// slot and first walk position from its bin's cursor with one 64-bit atomic (so the two stay
+// consistent and the walk positions increase with the slot).  Points past P are dropped here,
+// as the reference drops them.
+// ---------------------------------------------------------------------------------
+__device__ __forceinline__ bool survivor_bin(const BinArgs& a, uint32_t r, uint32_t points, uint32_t& g,
+                                             uint32_t& start, uint32_t& eff, uint32_t& bin) {
+    g = __ldg(a.surv_gid + r);
+    start = __ldg(a.surv_start + r);
+    if (start >= points) return false;
+    eff = min(__ldg(a.counts + g), points - start);
+    if (eff == 0u) return false;
+    const float2 pm = __ldg(reinterpret_cast<const float2*>(a.records + g));
+    const float x = fminf(fmaxf(pm.x, 0.0f), (float)(a.up_width - 1));   // NaN -> 0
+    const float y = fminf(fmaxf(pm.y, 0.0f), (float)(a.up_height - 1));
+    const int bx = min((int)x >> a.bin_shift, a.bins_x - 1);
+    const int by = min((int)y >> a.bin_shift, a.bins_y - 1);
+    bin = (uint32_t)(by * a.bins_x + bx);
+    return true;
+}
+
+__global__ void __launch_bounds__(256) bin_count_kernel(BinArgs a) {
+    const uint32_t survivors = a.counters->survivors, points = a.counters->points;
+    for (uint32_t r = blockIdx.x * blockDim.x + threadIdx.x; r < survivors; r += gridDim.x * blockDim.x) {
+        uint32_t g, start, eff, bin;
+        if (survivor_bin(a, r, points, g, start, eff, bin)) atomicAdd(a.bins + bin, (1ull << 32) | eff);
+    }
+}
+
+// One block: exclusive prefix of the bin words in place (rounds through shared memory, as in
+// scan_tiles_kernel); the binned survivor count goes to counters->pad[0].
+__global__ void __launch_bounds__(kTileScanThreads) bin_scan_kernel(BinArgs a) {
+    __shared__ unsigned long long words[kTileScanThreads * kTileScanPer];
+    constexpr uint32_t kRound = kTileScanThreads * kTileScanPer;
+    uint32_t carry_s = 0, carry_p = 0;
+    for (uint32_t r0 = 0; r0 < a.nbins; r0 += kRound) {
+        for (uint32_t i = threadIdx.x; i < kRound; i += kTileScanThreads)
+            words[i] = r0 + i < a.nbins ? a.bins[r0 + i] : 0ull;
+        __syncthreads();
+        uint32_t sv = 0, pt = 0;
+#pragma unroll
+        for (int k = 0; k < kTileScanPer; ++k) {
+            const unsigned long long v = words[threadIdx.x * kTileScanPer + k];
+            sv += (uint32_t)(v >> 32);
+            pt += (uint32_t)v;
+        }
+        uint32_t ex_s, ex_p, tot_s, tot_p;
+        block_scan_pair<kTileScanThreads>(sv, pt, ex_s, ex_p, tot_s, tot_p);
+        ex_s += carry_s;
+        ex_p += carry_p;
+#pragma unroll
+        for (int k = 0; k < kTileScanPer; ++k) {
+            const unsigned long long v = words[threadIdx.x * kTileScanPer + k];
+            words[threadIdx.x * kTileScanPer + k] = ((unsigned long long)ex_s << 32) | ex_p;
+            ex_s += (uint32_t)(v >> 32);
+            ex_p += (uint32_t)v;
+        }
+        __syncthreads();
+        for (uint32_t i = threadIdx.x; i < kRound && r0 + i < a.nbins; i += kTileScanThreads) a.bins[r0 + i] = words[i];
+        carry_s += tot_s;
+        carry_p += tot_p;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) a.counters->pad[0] = carry_s;
+}
+
+__global__ void __launch_bounds__(256) bin_scatter_kernel(BinArgs a) {
+    const uint32_t survivors = a.counters->survivors, points = a.counters->points;
+    for (uint32_t r = blockIdx.x * blockDim.x + threadIdx.x; r < survivors; r += gridDim.x * blockDim.x) {
+        uint32_t g, start, eff, bin;
+        if (!survivor_bin(a, r, points, g, start, eff, bin)) continue;
+        const unsigned long long old = atomicAdd(a.bins + bin, (1ull << 32) | eff);
+        const uint32_t slot = (uint32_t)(old >> 32);
+        a.sorted_gid[slot] = g;
+        a.sorted_pstart[slot] = start;
+        a.sorted_qstart[slot] = (uint32_t)old;
     }
 }
 
@@ -819,17 +909,20 @@ __global__ void __launch_bounds__(kSplatTile, kSplatRounds > 1 ? 4 : 1) splat_ke
     __shared__ uint32_t s_spread[kTileSize];
     if (GPS_SPLAT_MORTON_LUT && threadIdx.x < kTileSize) s_spread[threadIdx.x] = morton_spread(threadIdx.x);
     const uint32_t points = a.counters->points;
-    const uint32_t survivors = a.counters->survivors;
-    // splats point p0 + threadIdx.x of a tile whose survivor starts are in `starts`
-    auto splat_tile_point = [&](uint32_t p0, uint32_t r0, const uint32_t* starts, int window) {
-        const uint32_t p = p0 + threadIdx.x;
-        if (p < points && starts[0] <= p) {
-            int lo = 0, hi = window - 1;  // largest k with starts[k] <= p
+    const uint32_t survivors = a.point_base ? a.counters->pad[0] : a.counters->survivors;
+    // splats walk position q0 + threadIdx.x of a tile whose survivor starts are in `starts`
+    auto splat_tile_point = [&](uint32_t q0, uint32_t r0, const uint32_t* starts, int window) {
+        const uint32_t q = q0 + threadIdx.x;
+        if (q < points && starts[0] <= q) {
+            int lo = 0, hi = window - 1;  // largest k with starts[k] <= q
             while (lo < hi) {
                 int mid = (lo + hi + 1) >> 1;
-                if (starts[mid] <= p) lo = mid;
+                if (starts[mid] <= q) lo = mid;
                 else hi = mid - 1;
             }
+            // the reference's point index (the seed): the walk position itself in Gaussian
+            // order, the survivor's first point plus the offset in screen-bin order
+            const uint32_t p = a.point_base ? __ldg(&a.point_base[r0 + lo]) + (q - starts[lo]) : q;
             const uint32_t g = __ldg(&a.surv_gid[r0 + lo]);
             if (g < a.n) {  // always true unless the scan gave up (device_timeouts)
                 const float4* rp = reinterpret_cast<const float4*>(a.records + g);
@@ -1444,7 +1537,7 @@ static_assert(kScanTile == kScanTileGaussians, "scan tile size");
 // tile words a scan of n Gaussians may use (the small-tile count, an upper bound)
 uint32_t scan_tile_count(uint32_t n) { return (uint32_t)(((uint64_t)n + kScanTileSmall - 1) / kScanTileSmall); }
 
-void launch_scan(const ScanArgs& a, uint32_t scan_tiles, cudaStream_t stream) {
+void launch_scan(const ScanArgs& a, uint32_t scan_tiles, cudaStream_t stream, bool owners) {
     if (scan_tiles == 0 || a.n == 0) {
         cudaMemsetAsync(a.counters, 0, sizeof(PassCounters), stream);
         return;
@@ -1463,8 +1556,21 @@ void launch_scan(const ScanArgs& a, uint32_t scan_tiles, cudaStream_t stream) {
     const uint64_t max_tiles = ((uint64_t)a.max_points + a.tile_points - 1) / a.tile_points;
     const uint64_t want = (max_tiles + 255) / 256;
     const int owner_grid = (int)(want < 1184 ? (want ? want : 1) : 1184);  // 148 SMs x 8
-    launch_k(tile_owner_kernel, owner_grid, 256, 0, stream, a.surv_start, a.tile_first_rank, a.counters, a.tile_points,
-             a.mask_iter);
+    if (owners)
+        launch_k(tile_owner_kernel, owner_grid, 256, 0, stream, a.surv_start, a.tile_first_rank, a.counters,
+                 a.tile_points, a.mask_iter, (unsigned long long*)nullptr, 0u);
+}
+
+void launch_bin(const BinArgs& b, const ScanArgs& a, cudaStream_t stream) {
+    const int grid = 148 * 8;
+    launch_k(bin_count_kernel, grid, 256, 0, stream, b);
+    launch_k(bin_scan_kernel, 1, kTileScanThreads, 0, stream, b);
+    launch_k(bin_scatter_kernel, grid, 256, 0, stream, b);
+    const uint64_t max_tiles = ((uint64_t)a.max_points + a.tile_points - 1) / a.tile_points;
+    const uint64_t want = (max_tiles + 255) / 256;
+    const int owner_grid = (int)std::max<uint64_t>(1, std::min<uint64_t>(want, 148 * 8));
+    launch_k(tile_owner_kernel, owner_grid, 256, 0, stream, (const uint32_t*)b.sorted_qstart, a.tile_first_rank,
+             (const PassCounters*)b.counters, a.tile_points, a.mask_iter, b.bins, b.nbins);
 }
 
 template <int K>
@@ -1606,9 +1712,42 @@ static_assert(kNoAllocScanMaxGaussians / kScanTileSmall <= kNoAllocScanMaxTiles,
 static __device__ __align__(256) unsigned long long g_noalloc_scan_scratch[kNoAllocScanMaxTiles + 1];
 
 namespace {
-constexpr int kNoAllocMaxDevices = 64;
+// The array's device address belongs to the module as loaded into one CUDA context: a driver
+// API context other than the device's primary one, or the primary context re-created after
+// cudaDeviceReset, loads the module again at another address.  So the cache is keyed on the
+// current context's ID (cuCtxGetId: unique for the life of the process, never reused), fetched
+// through the runtime's driver entry points so the library needs no libcuda link.
+struct NoAllocScratchEntry {
+    unsigned long long ctx_id;
+    unsigned long long* ptr;
+};
+constexpr int kNoAllocCacheSlots = 64;
 std::mutex g_noalloc_mutex;
-unsigned long long* g_noalloc_scratch_ptr[kNoAllocMaxDevices] = {};
+NoAllocScratchEntry g_noalloc_cache[kNoAllocCacheSlots] = {};
+int g_noalloc_cache_next = 0;
+using CuCtxGetCurrentFn = int (*)(void**);
+using CuCtxGetIdFn = int (*)(void*, unsigned long long*);
+
+bool current_context_id(unsigned long long& id) {
+    static CuCtxGetCurrentFn get_current = nullptr;
+    static CuCtxGetIdFn get_id = nullptr;
+    if (!get_current || !get_id) {
+        void* f0 = nullptr;
+        void* f1 = nullptr;
+        cudaDriverEntryPointQueryResult q0, q1;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f0, cudaEnableDefault, &q0) != cudaSuccess ||
+            q0 != cudaDriverEntryPointSuccess || !f0)
+            return false;
+        if (cudaGetDriverEntryPoint("cuCtxGetId", &f1, cudaEnableDefault, &q1) != cudaSuccess ||
+            q1 != cudaDriverEntryPointSuccess || !f1)
+            return false;
+        get_current = reinterpret_cast<CuCtxGetCurrentFn>(f0);
+        get_id = reinterpret_cast<CuCtxGetIdFn>(f1);
+    }
+    void* ctx = nullptr;
+    if (get_current(&ctx) != 0 || !ctx) return false;
+    return get_id(ctx, &id) == 0;
+}
 }  // namespace
 
 }  // namespace gps
@@ -1634,25 +1773,41 @@ extern "C" gps_status gps_workload_scan_noalloc(const uint32_t* d_counts, const 
     }
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
-    if (e != cudaSuccess || dev < 0 || dev >= kNoAllocMaxDevices) {
+    if (e != cudaSuccess) {
         set_last_error(std::string("gps_workload_scan_noalloc: no usable current device: ") + cudaGetErrorString(e));
         return GPS_ERR_CUDA;
     }
-    unsigned long long* scratch;
+    // An error left pending by earlier, unrelated work is reported as such and left in place
+    // for the caller's own check; it is not taken for a failure of this scan.
+    e = cudaPeekAtLastError();
+    if (e != cudaSuccess) {
+        set_last_error(std::string("gps_workload_scan_noalloc: a CUDA error from earlier work is pending: ") +
+                       cudaGetErrorString(e));
+        return GPS_ERR_CUDA;
+    }
+    unsigned long long* scratch = nullptr;
     {
-        // Once per device, with that device current: the host-side name of a __device__
-        // array is not a device address, the address must be looked up.
+        // Once per context, with it current: the host-side name of a __device__ array is not a
+        // device address, the address must be looked up.
+        unsigned long long ctx_id = 0;
+        const bool have_id = current_context_id(ctx_id);
         std::lock_guard<std::mutex> lock(g_noalloc_mutex);
-        if (!g_noalloc_scratch_ptr[dev]) {
+        if (have_id)
+            for (const NoAllocScratchEntry& en : g_noalloc_cache)
+                if (en.ptr && en.ctx_id == ctx_id) scratch = en.ptr;
+        if (!scratch) {
             void* p = nullptr;
             e = cudaGetSymbolAddress(&p, g_noalloc_scan_scratch);
             if (e != cudaSuccess) {
                 set_last_error(std::string("gps_workload_scan_noalloc: cudaGetSymbolAddress failed: ") + cudaGetErrorString(e));
                 return GPS_ERR_CUDA;
             }
-            g_noalloc_scratch_ptr[dev] = static_cast<unsigned long long*>(p);
+            scratch = static_cast<unsigned long long*>(p);
+            if (have_id) {  // without a context ID the address is looked up on every call
+                g_noalloc_cache[g_noalloc_cache_next] = {ctx_id, scratch};
+                g_noalloc_cache_next = (g_noalloc_cache_next + 1) % kNoAllocCacheSlots;
+            }
         }
-        scratch = g_noalloc_scratch_ptr[dev];
     }
     cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
     ScanArgs a{};
@@ -1667,7 +1822,7 @@ extern "C" gps_status gps_workload_scan_noalloc(const uint32_t* d_counts, const 
     a.tile_state = scratch;
     a.counters = reinterpret_cast<PassCounters*>(d_counters8);
     launch_scan(a, tiles, st);  // writes every tile word and all eight counters
-    e = cudaGetLastError();
+    e = cudaGetLastError();  // nothing was pending before the launches: this is theirs
     if (e != cudaSuccess) {
         set_last_error(std::string("gps_workload_scan_noalloc: ") + cudaGetErrorString(e));
         return GPS_ERR_CUDA;

@@ -47,7 +47,9 @@ struct PassCounters {
     uint32_t points;       // min(total_points, max_number_of_points)
     uint32_t truncated;    // 1 if the point budget clipped the tail
     uint32_t scan_timeouts;  // always 0: no device-side wait can give up
-    uint32_t pad[3];
+    uint32_t loaded;         // Gaussians whose attributes the pass's preprocess read (after the
+                             // block cull and pass 2's previous-mask test); 0 without a tally
+    uint32_t pad[2];
 };
 
 struct FrameConst {
@@ -86,6 +88,7 @@ struct PreprocessArgs {
     // for the device-side pass counter it (see ScanArgs::mask_iter).
     uint32_t* mask_pair[2];
     const uint32_t* mask_iter;
+    uint32_t* loaded;             // tally of Gaussians whose attributes were read (null: none)
 };
 
 struct ScanArgs {
@@ -105,6 +108,7 @@ struct ScanArgs {
     uint32_t* tile_first_rank;   // [ceil(max_points / tile_points) + 1]
     unsigned long long* tile_state;  // [scan tiles] tile totals, then tile prefixes
     PassCounters* counters;
+    uint32_t* loaded;            // the preprocess's tally: moved into counters->loaded and reset
 };
 
 struct SplatArgs {
@@ -112,11 +116,38 @@ struct SplatArgs {
     int frame_seed;
     const SplatRecord* records;
     const uint32_t* surv_gid;
-    const uint32_t* surv_start;
+    const uint32_t* surv_start;      // first walk position of each survivor (monotone)
     const uint32_t* tile_first_rank;
     const PassCounters* counters;
     uint64_t* buffer;
     uint32_t n;
+    // Screen-binned order (null: Gaussian order, where a walk position is the point index):
+    // survivor i's points are the reference's point indices point_base[i] + (q - surv_start[i]).
+    const uint32_t* point_base;
+};
+
+// Screen-tile binning of one pass's survivors: the splat walks survivors grouped by the 64x64
+// splat-buffer tile (or block of tiles) holding their pixel mean, so that blocks running at the
+// same time write a compact part of the buffer.  Only the order changes: every point keeps its
+// reference point index (its seed) and the min is order-free.
+constexpr uint32_t kMaxBins = 16384;  // screen bins per pass (bins widen beyond 8192 x 8192 pixels)
+#ifndef GPS_SPLAT_BINNED
+#define GPS_SPLAT_BINNED 0
+#endif
+struct BinArgs {
+    const SplatRecord* records;
+    const uint32_t* surv_gid;        // Gaussian order (the scan's output)
+    const uint32_t* surv_start;      // first point (reference point index) per survivor
+    const uint32_t* counts;
+    PassCounters* counters;          // survivors and P in; binned survivors out (pad[0])
+    unsigned long long* bins;        // [nbins + 1] (survivors << 32 | points): counts, then cursors
+    uint32_t nbins;
+    int bins_x, bins_y;              // bin grid
+    int bin_shift;                   // log2 of the bin width in pixels (6 = one buffer tile)
+    int up_width, up_height;
+    uint32_t* sorted_gid;            // [n] outputs in bin order
+    uint32_t* sorted_pstart;
+    uint32_t* sorted_qstart;
 };
 
 struct ResolveArgs {
@@ -146,7 +177,9 @@ void launch_encode_half(const float4* pos_op, const float4* rot, const float4* s
 void launch_translate_origins(const float4* src, uint32_t count, float dx, float dz, float4* dst, cudaStream_t stream);
 void launch_tile_nodes(const float4* src, uint32_t src_pb, uint32_t src_n, uint32_t pb, uint32_t copies,
                        const float2* offsets, uint64_t total, float4* dst, uint32_t nodes, cudaStream_t stream);
-void launch_scan(const ScanArgs& a, uint32_t scan_tiles, cudaStream_t stream);
+void launch_scan(const ScanArgs& a, uint32_t scan_tiles, cudaStream_t stream, bool owners = true);
+// screen-bin the scanned survivors and find each splat tile's first survivor in that order
+void launch_bin(const BinArgs& b, const ScanArgs& a, cudaStream_t stream);
 uint32_t scan_tile_count(uint32_t n);
 constexpr uint32_t kScanTileGaussians = 16384;  // Gaussians per scan tile (counts are padded to it)
 void launch_splat(const SplatArgs& a, int grid, int block, cudaStream_t stream);

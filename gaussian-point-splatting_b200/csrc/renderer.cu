@@ -244,9 +244,11 @@ struct gps_renderer {
     uint64_t entries = 0;
     uint32_t n = 0, n_pad = 0;
     dptr<uint64_t> buffer;
-    dptr<uint32_t> counts, mask[2], surv_gid, surv_start, tile_first_rank, culled, chunk_list, chunk_count;
+    dptr<uint32_t> counts, mask[2], surv_gid, surv_start, tile_first_rank, culled, chunk_list, chunk_count, loaded;
     dptr<SplatRecord> records;
     dptr<unsigned long long> tile_state;
+    dptr<unsigned long long> bins;  // screen-bin histogram / cursors, kMaxBins + 1 words
+    dptr<uint32_t> sorted_gid, sorted_pstart, sorted_qstart;  // survivors in screen-bin order
     dptr<PassCounters> counters;  // [2]: pass 1, pass 2
     dptr<float> mip;
     dptr<unsigned> hiz_done;
@@ -366,6 +368,7 @@ void render_pass(gps_renderer* r, const FrameConst& fc, int frame, bool first, c
     pa.chunk_count = listed ? r->chunk_count.get() : nullptr;
     pa.immediate_threshold = r->s.immediate_splat_threshold;
     pa.buffer = r->buffer.get();
+    pa.loaded = r->loaded.get();
     if (r->scene->format == GPS_SCENE_FP32) {
         SceneFP32 s{r->scene->pos_op.get(), r->scene->rot.get(), r->scene->scale.get(), r->scene->sh.get(), r->n};
         launch_preprocess_fp32(pa, s, st);
@@ -398,15 +401,43 @@ void render_pass(gps_renderer* r, const FrameConst& fc, int frame, bool first, c
     sa.tile_first_rank = r->tile_first_rank.get();
     sa.tile_state = r->tile_state.get();
     sa.counters = pc;
-    launch_scan(sa, r->scan_tiles, st);
-    count_launch(r, kStScan, r->scan_tiles ? 4 : 0);  // tile reduce, tile scan, downsweep, tile owners
+    sa.loaded = r->loaded.get();
+    const bool binned = GPS_SPLAT_BINNED != 0;
+    launch_scan(sa, r->scan_tiles, st, !binned);
+    count_launch(r, kStScan, r->scan_tiles ? 3 : 0);  // tile reduce, tile scan, downsweep
+    BinArgs b{};
+    if (binned) {
+        b.records = r->records.get();
+        b.surv_gid = r->surv_gid.get();
+        b.surv_start = r->surv_start.get();
+        b.counts = r->counts.get();
+        b.counters = pc;
+        b.bins = r->bins.get();
+        b.up_width = fc.up_width;
+        b.up_height = fc.up_height;
+        b.bin_shift = 6;  // one 64x64 splat-buffer tile per bin, coarser for very large views
+        while ((uint64_t)((fc.up_width + (1 << b.bin_shift) - 1) >> b.bin_shift) *
+                   (uint64_t)((fc.up_height + (1 << b.bin_shift) - 1) >> b.bin_shift) > kMaxBins)
+            ++b.bin_shift;
+        b.bins_x = (fc.up_width + (1 << b.bin_shift) - 1) >> b.bin_shift;
+        b.bins_y = (fc.up_height + (1 << b.bin_shift) - 1) >> b.bin_shift;
+        b.nbins = (uint32_t)(b.bins_x * b.bins_y);
+        b.sorted_gid = r->sorted_gid.get();
+        b.sorted_pstart = r->sorted_pstart.get();
+        b.sorted_qstart = r->sorted_qstart.get();
+        launch_bin(b, sa, st);
+        count_launch(r, kStScan, 4);  // bin count, bin scan, bin scatter, tile owners
+    } else {
+        count_launch(r, kStScan, r->scan_tiles ? 1 : 0);  // tile owners
+    }
     r->timer.mark(kStSplat, st);
     SplatArgs sp{};
     sp.fc = fc;
     sp.frame_seed = frame_seed + 1;
     sp.records = r->records.get();
-    sp.surv_gid = r->surv_gid.get();
-    sp.surv_start = r->surv_start.get();
+    sp.surv_gid = binned ? r->sorted_gid.get() : r->surv_gid.get();
+    sp.surv_start = binned ? r->sorted_qstart.get() : r->surv_start.get();
+    sp.point_base = binned ? r->sorted_pstart.get() : nullptr;
     sp.tile_first_rank = r->tile_first_rank.get();
     sp.counters = pc;
     sp.buffer = r->buffer.get();
@@ -712,6 +743,11 @@ gps_status create_renderer(gps_scene* scene, const gps_settings* settings, const
         r->records.reset(dev_alloc<SplatRecord>(std::max<uint32_t>(r->n, 1)));
         r->surv_gid.reset(dev_alloc<uint32_t>(std::max<uint32_t>(r->n, 1)));
         r->surv_start.reset(dev_alloc<uint32_t>(std::max<uint32_t>(r->n, 1)));
+        r->sorted_gid.reset(dev_alloc<uint32_t>(std::max<uint32_t>(r->n, 1)));
+        r->sorted_pstart.reset(dev_alloc<uint32_t>(std::max<uint32_t>(r->n, 1)));
+        r->sorted_qstart.reset(dev_alloc<uint32_t>(std::max<uint32_t>(r->n, 1)));
+        r->bins.reset(dev_alloc<unsigned long long>(kMaxBins + 1));
+        GPS_CUDA(cudaMemset(r->bins.get(), 0, sizeof(unsigned long long) * (kMaxBins + 1)));
         const uint64_t max_pts = (uint64_t)std::max(0, s.max_number_of_points);
         r->tile_first_rank.reset(dev_alloc<uint32_t>(max_pts / 256 + 2));
         r->tile_state.reset(dev_alloc<unsigned long long>(std::max<uint32_t>(r->scan_tiles, 1)));
@@ -722,6 +758,8 @@ gps_status create_renderer(gps_scene* scene, const gps_settings* settings, const
         r->chunk_list.reset(dev_alloc<uint32_t>(words + 1));
         r->chunk_count.reset(dev_alloc<uint32_t>(1));
         GPS_CUDA(cudaMemset(r->chunk_count.get(), 0, sizeof(uint32_t)));
+        r->loaded.reset(dev_alloc<uint32_t>(1));
+        GPS_CUDA(cudaMemset(r->loaded.get(), 0, sizeof(uint32_t)));
         GPS_CUDA(cudaMemset(r->culled.get(), 0, sizeof(uint32_t) * (bwords + 1)));
         hiz_layout(r->hiz, s.width, s.height);
         r->cap_mip = std::max(r->hiz.mip_size, cap_hiz.mip_size);
@@ -865,6 +903,8 @@ gps_status gps_renderer_stats(gps_renderer* r, gps_stats* out) {
     out->truncated = (int32_t)(c[0].truncated | c[1].truncated);
     out->device_timeouts = (int32_t)(c[0].scan_timeouts + c[1].scan_timeouts);
     out->kernel_launches = (int32_t)r->frame_launches;
+    out->gaussians_read_one = (int32_t)c[0].loaded;
+    out->gaussians_read_two = (int32_t)c[1].loaded;
     if (out->device_timeouts) return fail(GPS_ERR_DEVICE_TIMEOUT, "a device-side look-back wait gave up");
     return GPS_OK;
 }

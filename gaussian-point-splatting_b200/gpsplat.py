@@ -126,6 +126,8 @@ class Stats(ctypes.Structure):
         ("truncated", c_int32),
         ("device_timeouts", c_int32),
         ("kernel_launches", c_int32),
+        ("gaussians_read_one", c_int32),
+        ("gaussians_read_two", c_int32),
     ]
 
 

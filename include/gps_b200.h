@@ -110,6 +110,9 @@ typedef struct gps_stats {
     int32_t truncated;                              /* 1 if the point budget clipped a pass */
     int32_t device_timeouts;                        /* bounded waits that gave up (0 normally) */
     int32_t kernel_launches;                        /* kernels the last frame launched */
+    int32_t gaussians_read_one, gaussians_read_two; /* Gaussians whose attributes the preprocess
+                                                       read per pass (after the block cull and
+                                                       pass 2's previous-mask test) */
 } gps_stats;
 
 typedef struct gps_scene gps_scene;
@@ -217,10 +220,14 @@ gps_status gps_renderer_debug_view(gps_renderer* r, gps_debug_view* out);
  *   d_tile_first_rank   output, max_points / 256 + 2 entries: first survivor of each 256-point tile
  *   d_counters8         output, 8 words: survivors, total points (mod 2^32),
  *                       points = min(total, max_points), truncated flag, 0, 0, 0, 0
- * The first call on a device looks the scratch array's address up (make it before any stream
- * capture on that device).  All calls on a device share the array; each call writes every word
- * of it that it reads before reading it, and calls that overlap on the GPU race on it —
- * serialise them (one stream at a time). */
+ * The first call in a CUDA context (the device's primary context, or a driver-API context
+ * made current by the caller) looks the scratch array's address up in that context and keeps
+ * it, keyed on the context's unique ID; make that first call before any stream capture.  A
+ * context re-created after cudaDeviceReset is a new context and gets its own lookup.  An
+ * error already pending from earlier work is reported (GPS_ERR_CUDA) and left pending.  All
+ * calls in a context share the array; each call writes every word of it that it reads before
+ * reading it, and calls that overlap on the GPU race on it — serialise them (one stream at a
+ * time). */
 gps_status gps_workload_scan_noalloc(const uint32_t* d_counts, const uint32_t* d_mask, uint32_t n,
                                      uint32_t max_points, uint32_t* d_surv_gid, uint32_t* d_surv_start,
                                      uint32_t* d_tile_first_rank, uint32_t* d_counters8, void* stream);

@@ -367,19 +367,27 @@ struct Ctx {
     uint32_t pts_pass[2] = {0, 0};
 };
 
+// Dynamic chunks (about 64 per thread) taken from a shared counter: the work per item is very
+// uneven (a survivor's point count, a culled vs visible chunk), so equal static ranges leave
+// most threads idle behind the densest one.
 template <class F>
 void par_for(int threads, size_t n, F f) {
     if (threads <= 1 || n < 1024) {
         f(0, n);
         return;
     }
+    const size_t grain = std::max<size_t>(16, n / ((size_t)threads * 64));
+    std::atomic<size_t> next{0};
+    auto worker = [&]() {
+        for (;;) {
+            const size_t b = next.fetch_add(grain, std::memory_order_relaxed);
+            if (b >= n) return;
+            f(b, std::min(n, b + grain));
+        }
+    };
     std::vector<std::thread> ts;
-    size_t chunk = (n + threads - 1) / threads;
-    for (int t = 0; t < threads; ++t) {
-        size_t b = (size_t)t * chunk, e = std::min(n, b + chunk);
-        if (b >= e) break;
-        ts.emplace_back([=]() { f(b, e); });
-    }
+    for (int t = 1; t < threads; ++t) ts.emplace_back(worker);
+    worker();
     for (auto& t : ts) t.join();
 }
 

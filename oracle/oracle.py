@@ -121,6 +121,61 @@ class Oracle:
             pass
 
 
+def settings_host(**overrides):
+    """A gps_settings with the reference's defaults (render_settings.cuh:36-265), filled here so
+    that the CPU baseline never loads the CUDA library; only the struct layout is shared."""
+    import gpsplat  # the ctypes struct definitions only; the shared library is not loaded
+
+    st = gpsplat.Settings()
+    d = dict(width=1920, height=1080, supersampling_factor=2, samples_per_pixel=1, max_number_of_points=250_000_000,
+             fovy=45.0, near_view_plane=0.2, far_view_plane=10000.0, enable_hierarchical_culling=1,
+             fully_disable_hierarchical_culling=0, enable_occlusion_culling=1, occlusion_culling_min_reduce_count=0,
+             cull_small_gaussians=0, use_unbiased_2d_splatting=1, reduce_point_count=1, accumulation_mode=0,
+             sort_morton_order=0, immediate_splat_threshold=0)
+    d.update(overrides)
+    for k, v in d.items():
+        if k == "background":
+            for i in range(3):
+                st.background[i] = float(v[i])
+        else:
+            setattr(st, k, v)
+    return st
+
+
+def camera_host(position, c2w, settings, frame: int):
+    """The viewer's per-frame camera (main.cu:141-157, camera.cpp:88-156) in numpy: view =
+    diag(1,-1,-1,1) * inverse([R | p]) with R the camera-to-world rotation (columns right, down,
+    forward), glm::perspective with NDC z in [-1, 1], normalised frustum planes of proj*view.
+    Float64 arithmetic rounded to float32: the CPU baseline's cameras, not the parity path's."""
+    import gpsplat
+
+    R = np.asarray(c2w, np.float64)
+    M = np.eye(4)
+    M[:3, :3] = R
+    M[:3, 3] = np.asarray(position, np.float64)
+    view = np.diag([1.0, -1.0, -1.0, 1.0]) @ np.linalg.inv(M)
+    f = 1.0 / np.tan(np.radians(settings.fovy) / 2.0)
+    aspect = settings.width / settings.height
+    n, fa = settings.near_view_plane, settings.far_view_plane
+    proj = np.zeros((4, 4))
+    proj[0, 0] = f / aspect
+    proj[1, 1] = f
+    proj[2, 2] = -(fa + n) / (fa - n)
+    proj[2, 3] = -2.0 * fa * n / (fa - n)
+    proj[3, 2] = -1.0
+    vp = proj @ view
+    planes = np.stack([vp[3] + vp[0], vp[3] - vp[0], vp[3] + vp[1], vp[3] - vp[1], vp[3] + vp[2], vp[3] - vp[2]])
+    planes /= np.linalg.norm(planes[:, :3], axis=1, keepdims=True)
+    cam = gpsplat.Camera()
+    cam.view[:] = [float(x) for x in view.T.astype(np.float32).reshape(-1)]
+    cam.proj[:] = [float(x) for x in proj.T.astype(np.float32).reshape(-1)]
+    cam.position[:] = [float(x) for x in np.asarray(position, np.float32)]
+    cam.frustum_planes[:] = [float(x) for x in planes.astype(np.float32).reshape(-1)]
+    cam.frame = int(frame)
+    cam.camera_moved = 1
+    return cam
+
+
 def kat(idx, frame, x):
     idx = np.ascontiguousarray(idx, np.uint32)
     frame = np.ascontiguousarray(frame, np.uint32)

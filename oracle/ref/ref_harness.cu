@@ -98,6 +98,50 @@ static void put_mat4(std::vector<float>& out, const glm::mat4& m) {
         for (int r = 0; r < 4; ++r) out.push_back(m[c][r]);
 }
 
+// temporalRender (post_processing_kernels.cuh:222-285) blends each pixel in place while its
+// neighbours read the same buffer for the 3x3 clamp, so its output depends on thread order.
+// This runs the UNMODIFIED kernel so that no read can see a blended value: nine launches, one
+// per pixel class (x mod 3, y mod 3), each on a fresh copy of the unblended colour buffer and
+// with NaN current depth everywhere outside the class.  A NaN depth reprojects to NaN, fails
+// the kernel's bounds test and writes the pixel's own unchanged colour back; pixels of one
+// class are at least 3 apart, so none reads another's blended value.  The class pixels of the
+// nine launches are assembled into the colour buffer and the u8 image.
+static void temporal_render_race_free(unsigned char* d_u8, glm::vec3* d_cur, const glm::vec3* d_prev, const float* d_cur_depth,
+                                      const float* d_prev_depth, const glm::mat4& reprojection, int W, int H, int frame_number) {
+    const size_t npx = size_t(W) * H;
+    std::vector<glm::vec3> pre(npx), out(npx);
+    std::vector<float> depth(npx), masked(npx);
+    std::vector<unsigned char> u8(npx * 3), u8_out(npx * 3);
+    cudaMemcpy(pre.data(), d_cur, npx * sizeof(glm::vec3), cudaMemcpyDeviceToHost);
+    cudaMemcpy(depth.data(), d_cur_depth, npx * sizeof(float), cudaMemcpyDeviceToHost);
+    float* d_masked = nullptr;
+    cudaMalloc(&d_masked, npx * sizeof(float));
+    dim3 block(256), grid((unsigned)((npx + 255) / 256));
+    for (int cls = 0; cls < 9; ++cls) {
+        const int cx = cls % 3, cy = cls / 3;
+        for (int y = 0; y < H; ++y)
+            for (int x = 0; x < W; ++x)
+                masked[size_t(y) * W + x] = (x % 3 == cx && y % 3 == cy) ? depth[size_t(y) * W + x] : NAN;
+        cudaMemcpy(d_masked, masked.data(), npx * sizeof(float), cudaMemcpyHostToDevice);
+        cudaMemcpy(d_cur, pre.data(), npx * sizeof(glm::vec3), cudaMemcpyHostToDevice);
+        temporalRender<<<grid, block>>>(d_u8, d_cur, d_prev, d_masked, d_prev_depth, reprojection, 0.9f, W, H, frame_number);
+        std::vector<glm::vec3> got(npx);
+        cudaMemcpy(got.data(), d_cur, npx * sizeof(glm::vec3), cudaMemcpyDeviceToHost);
+        cudaMemcpy(u8.data(), d_u8, npx * 3, cudaMemcpyDeviceToHost);
+        for (int y = cy; y < H; y += 3)
+            for (int x = cx; x < W; x += 3) {
+                const size_t i = size_t(y) * W + x;
+                out[i] = got[i];
+                u8_out[3 * i + 0] = u8[3 * i + 0];
+                u8_out[3 * i + 1] = u8[3 * i + 1];
+                u8_out[3 * i + 2] = u8[3 * i + 2];
+            }
+    }
+    cudaMemcpy(d_cur, out.data(), npx * sizeof(glm::vec3), cudaMemcpyHostToDevice);
+    cudaMemcpy(d_u8, u8_out.data(), npx * 3, cudaMemcpyHostToDevice);
+    cudaFree(d_masked);
+}
+
 static int run_render(int argc, char** argv) {
     if (argc < 5) { fprintf(stderr, "usage: render <ply> <outdir> <camfile> [opts]\n"); return 2; }
     std::string ply = argv[2], outdir = argv[3], camfile = argv[4];
@@ -108,6 +152,7 @@ static int run_render(int argc, char** argv) {
     int frames_to_dump = 1 << 30;
     bool dump_full = true, timing = false, dump_post = true;
     int warmup = 0;
+    bool taa_race_free = false;
     for (int i = 5; i < argc; ++i) {
         std::string a = argv[i];
         if (a == "--res") { s.resolution.x = atoi(argv[++i]); s.resolution.y = atoi(argv[++i]); }
@@ -126,6 +171,7 @@ static int run_render(int argc, char** argv) {
         else if (a == "--min-reduce") s.occlusion_culling_min_reduce_count = atoi(argv[++i]);
         else if (a == "--background") { s.backgroundColor.x = (float)atof(argv[++i]); s.backgroundColor.y = (float)atof(argv[++i]); s.backgroundColor.z = (float)atof(argv[++i]); }
         else if (a == "--taa") s.accumulationMode = AccumulationMode::TAA;
+        else if (a == "--taa-race-free") { s.accumulationMode = AccumulationMode::TAA; taa_race_free = true; }
         else if (a == "--no-accumulation") s.accumulationMode = AccumulationMode::None;
         else if (a == "--sort-morton-order") s.sort_morton_order = true;
         else if (a == "--immediate-threshold") s.immediate_splat_threshold = atoi(argv[++i]);
@@ -218,8 +264,12 @@ static int run_render(int argc, char** argv) {
                 numProgressiveFrames++;
                 glm::mat4 modelMat = glm::affineInverse(s.cameraViewMatrix);
                 glm::mat4 deltaMatrix = s.previousViewProjectionMatrix * modelMat * glm::inverse(s.cameraProjectionMatrix);
-                temporalRender<<<gridSize, blockSize>>>(d_u8, d_color[a], d_color[b], d_depth[a], d_depth[b],
-                                                        deltaMatrix, 0.9f, W, H, numProgressiveFrames);
+                if (taa_race_free)
+                    temporal_render_race_free(d_u8, d_color[a], d_color[b], d_depth[a], d_depth[b], deltaMatrix, W, H,
+                                              numProgressiveFrames);
+                else
+                    temporalRender<<<gridSize, blockSize>>>(d_u8, d_color[a], d_color[b], d_depth[a], d_depth[b],
+                                                            deltaMatrix, 0.9f, W, H, numProgressiveFrames);
             } else {
                 if (s.cameraMoved || s.accumulationMode == AccumulationMode::None) numProgressiveFrames = 1;
                 else numProgressiveFrames++;
@@ -444,6 +494,172 @@ static int run_probe(int argc, char** argv) {
 }
 
 // ---------------------------------------------------------------------------------
+// One point's samples through the reference's device functions (loadAndTransformGaussian,
+// Random::pcg2d / correctedBoxMuller, the splatGaussianPoint position expression), with the
+// intermediates written out: 12 floats per sample (parity debugging).
+// ---------------------------------------------------------------------------------
+__global__ void sample_probe_kernel(GPUGaussianScene scene, uint32_t g, uint32_t point, int frame_seed, glm::mat4 vp,
+                                    glm::mat4 v, glm::vec2 tan_fov, glm::vec2 focal, int upw, int uph, int ss,
+                                    int samples, float* out) {
+    if (blockIdx.x != 0 || threadIdx.x != 0) return;
+    GaussianGeometry gg;
+    glm::vec4 proj_mean;
+    glm::vec2 pixel_mean;
+    glm::vec3 cov2d;
+    glm::ivec2 mn, mx;
+    float det = 0, view_z = 0;
+    if (!loadAndTransformGaussian(scene, g, vp, v, tan_fov, focal, upw, uph, ss, gg, proj_mean, pixel_mean, cov2d, mn, mx,
+                                  det, view_z))
+        return;
+    const float opacity = scene.get_opacity(g);
+    const float c0 = __fsqrt_rn(cov2d.x);
+    const float c1 = cov2d.y / c0;
+    const float c2 = __fsqrt_rn(cov2d.z - c1 * c1);
+    uint2 seed = Random::makeSeed(point, frame_seed);
+    for (int q = 0; q < samples; ++q) {
+        float2 u = Random::pcg2d(seed);
+        float2 xy = Random::correctedBoxMuller(u.x, u.y, opacity);
+        glm::vec2 pixel(pixel_mean.x + c0 * xy.x, pixel_mean.y + c1 * xy.x + c2 * xy.y);
+        float* o = out + 12 * q;
+        o[0] = u.x; o[1] = u.y; o[2] = xy.x; o[3] = xy.y; o[4] = pixel.x; o[5] = pixel.y;
+        o[6] = pixel_mean.x; o[7] = pixel_mean.y; o[8] = c0; o[9] = c1; o[10] = c2; o[11] = opacity;
+    }
+}
+
+static int run_sample_probe(int argc, char** argv) {
+    if (argc < 8) { fprintf(stderr, "usage: sampleprobe <ply> <outdir> <camfile> <gaussian> <point> <frame_seed> [opts]\n"); return 2; }
+    RenderSettings s;
+    s.statistics = new Statistics();
+    s.model_path = argv[2];
+    std::string outdir = argv[3];
+    std::vector<CamRecord> cams;
+    {
+        std::ifstream f(argv[4], std::ios::binary);
+        CamRecord r;
+        while (f.read(reinterpret_cast<char*>(&r), sizeof(r))) cams.push_back(r);
+    }
+    const uint32_t g = (uint32_t)strtoul(argv[5], nullptr, 10);
+    const uint32_t point = (uint32_t)strtoul(argv[6], nullptr, 10);
+    const int frame_seed = atoi(argv[7]);
+    for (int i = 8; i < argc; ++i) {
+        std::string a = argv[i];
+        if (a == "--res") { s.resolution.x = atoi(argv[++i]); s.resolution.y = atoi(argv[++i]); }
+        else if (a == "--ss") s.supersampling_factor = atoi(argv[++i]);
+        else if (a == "--spp") s.render_pass_count = atoi(argv[++i]);
+        else if (a == "--fovy") s.fovy = (float)atof(argv[++i]);
+    }
+    if (cams.empty()) return 2;
+    GaussianPointSplatting* gps = new GaussianPointSplatting(s);
+    if (g >= (uint32_t)gps->numGaussians) { fprintf(stderr, "gaussian out of range\n"); return 2; }
+    const CamRecord& c = cams[0];
+    s.cameraViewMatrix = to_mat4(c.view);
+    s.cameraProjectionMatrix = to_mat4(c.proj);
+    auto vMatrix = s.cameraViewMatrix;
+    auto vpMatrix = s.cameraProjectionMatrix * vMatrix;
+    float r = s.get_aspectXY();
+    float t_f_y = glm::tan(glm::radians(s.fovy) * 0.5f);
+    float fovx = 2.0f * glm::atan(t_f_y * r);
+    float t_f_x = glm::tan(fovx * 0.5f);
+    glm::vec2 tan_fov{ t_f_x, t_f_y };
+    glm::vec2 focal{ s.resolution.x * s.supersampling_factor / (2.0f * tan_fov.x),
+                     s.resolution.y * s.supersampling_factor / (2.0f * tan_fov.y) };
+    const int samples = s.render_pass_count * s.supersampling_factor * s.supersampling_factor;
+    float* d_out;
+    cudaMalloc(&d_out, sizeof(float) * 12 * samples);
+    cudaMemset(d_out, 0, sizeof(float) * 12 * samples);
+    sample_probe_kernel<<<1, 32>>>(gps->gpuGaussianScene, g, point, frame_seed, vpMatrix, vMatrix, tan_fov, focal,
+                                   s.resolution.x * s.supersampling_factor, s.resolution.y * s.supersampling_factor,
+                                   s.supersampling_factor, samples, d_out);
+    cudaDeviceSynchronize();
+    std::vector<float> out = d2h(d_out, (size_t)12 * samples);
+    write_npy(outdir + "/sample_probe.npy", out.data(), out.size(), "<f4", 4, {(size_t)samples, 12});
+    cudaError_t err = cudaGetLastError();
+    if (err != cudaSuccess) { fprintf(stderr, "CUDA error: %s\n", cudaGetErrorString(err)); return 3; }
+    return 0;
+}
+
+// ---------------------------------------------------------------------------------
+// The reference's own splat kernel (splatGaussianPointsKernel, unmodified) over a given
+// point -> Gaussian index array and frame seed, into a freshly cleared buffer: where exactly
+// the reference puts the samples of chosen points (parity debugging).  Writes the entries that
+// differ from the clear value as (index, value) pairs.
+// ---------------------------------------------------------------------------------
+static int run_splat_points(int argc, char** argv) {
+    if (argc < 7) { fprintf(stderr, "usage: splatpoints <ply> <outdir> <camfile> <indices.u32> <frame_seed> [opts]\n"); return 2; }
+    RenderSettings s;
+    s.statistics = new Statistics();
+    s.model_path = argv[2];
+    std::string outdir = argv[3];
+    std::vector<CamRecord> cams;
+    {
+        std::ifstream f(argv[4], std::ios::binary);
+        CamRecord r;
+        while (f.read(reinterpret_cast<char*>(&r), sizeof(r))) cams.push_back(r);
+    }
+    std::vector<uint32_t> ids;
+    {
+        std::ifstream f(argv[5], std::ios::binary);
+        uint32_t v;
+        while (f.read(reinterpret_cast<char*>(&v), 4)) ids.push_back(v);
+    }
+    const int frame_seed = atoi(argv[6]);
+    for (int i = 7; i < argc; ++i) {
+        std::string a = argv[i];
+        if (a == "--res") { s.resolution.x = atoi(argv[++i]); s.resolution.y = atoi(argv[++i]); }
+        else if (a == "--ss") s.supersampling_factor = atoi(argv[++i]);
+        else if (a == "--spp") s.render_pass_count = atoi(argv[++i]);
+        else if (a == "--fovy") s.fovy = (float)atof(argv[++i]);
+        else if (a == "--near") s.near_view_plane = (float)atof(argv[++i]);
+        else if (a == "--far") s.far_view_plane = (float)atof(argv[++i]);
+    }
+    if (cams.empty() || ids.empty()) return 2;
+    GaussianPointSplatting* gps = new GaussianPointSplatting(s);
+    if (ids.size() > 0) {
+        uint32_t mx = 0;
+        for (uint32_t v : ids) mx = v > mx ? v : mx;
+        if (mx >= (uint32_t)gps->numGaussians) { fprintf(stderr, "index %u out of range\n", mx); return 2; }
+    }
+    const CamRecord& c = cams[0];
+    s.cameraViewMatrix = to_mat4(c.view);
+    s.cameraProjectionMatrix = to_mat4(c.proj);
+    auto vMatrix = s.cameraViewMatrix;
+    auto camMatrix = glm::affineInverse(vMatrix);
+    auto vpMatrix = s.cameraProjectionMatrix * vMatrix;
+    float r = s.get_aspectXY();
+    float t_f_y = glm::tan(glm::radians(s.fovy) * 0.5f);
+    float fovx = 2.0f * glm::atan(t_f_y * r);
+    float t_f_x = glm::tan(fovx * 0.5f);
+    glm::vec2 tan_fov{ t_f_x, t_f_y };
+    glm::vec2 focal{ s.resolution.x * s.supersampling_factor / (2.0f * tan_fov.x),
+                     s.resolution.y * s.supersampling_factor / (2.0f * tan_fov.y) };
+    const int upw = s.resolution.x * s.supersampling_factor, uph = s.resolution.y * s.supersampling_factor;
+    const size_t tiles = size_t((upw + 63) / 64) * size_t((uph + 63) / 64);
+    const size_t entries = tiles * 4096 * size_t(s.render_pass_count);
+    const uint64_t clear = 0xFFFFFFF000000000ull;
+    std::vector<uint64_t> init(entries, clear);
+    uint64_t* d_buf;
+    uint32_t* d_ids;
+    cudaMalloc(&d_buf, entries * 8);
+    cudaMalloc(&d_ids, ids.size() * 4);
+    cudaMemcpy(d_buf, init.data(), entries * 8, cudaMemcpyHostToDevice);
+    cudaMemcpy(d_ids, ids.data(), ids.size() * 4, cudaMemcpyHostToDevice);
+    const int n = (int)ids.size();
+    splatGaussianPointsKernel<<<(n + 255) / 256, 256>>>(gps->gpuGaussianScene, d_ids, d_buf, vpMatrix, vMatrix, camMatrix,
+                                                       tan_fov, focal, upw, uph, s.render_pass_count, frame_seed, n,
+                                                       s.near_view_plane, s.far_view_plane, s.use_unbiased_2d_splatting,
+                                                       s.reduce_point_count, s.supersampling_factor);
+    cudaDeviceSynchronize();
+    std::vector<uint64_t> buf = d2h(d_buf, entries);
+    std::vector<uint64_t> pairs;
+    for (size_t i = 0; i < entries; ++i)
+        if (buf[i] != clear) { pairs.push_back(i); pairs.push_back(buf[i]); }
+    write_npy(outdir + "/splat_points.npy", pairs.data(), pairs.size(), "<u8", 8, {pairs.size() / 2, 2});
+    cudaError_t err = cudaGetLastError();
+    if (err != cudaSuccess) { fprintf(stderr, "CUDA error: %s\n", cudaGetErrorString(err)); return 3; }
+    return 0;
+}
+
+// ---------------------------------------------------------------------------------
 // Known-answer vectors from the reference's device helpers
 // ---------------------------------------------------------------------------------
 __global__ void kat_kernel(const uint32_t* idx, const uint32_t* frame, const float* fin, int n,
@@ -599,6 +815,8 @@ int main(int argc, char** argv) {
     if (mode == "kat") return run_kat(argc, argv);
     if (mode == "camera") return run_camera(argc, argv);
     if (mode == "probe") return run_probe(argc, argv);
+    if (mode == "splatpoints") return run_splat_points(argc, argv);
+    if (mode == "sampleprobe") return run_sample_probe(argc, argv);
     fprintf(stderr, "unknown mode %s\n", mode.c_str());
     return 2;
 }

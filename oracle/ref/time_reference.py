@@ -62,7 +62,7 @@ def main():
         cams = gpsutil.cameras_for(s, [(p, synth.look_at_c2w(p, [0.0, 0.0, 0.0]))] * total)
     camf = os.path.join(work, "cams.bin")
     gpsutil.write_camera_file(camf, cams)
-    res = subprocess.run([exe, "render", ply, work, camf] + gpsutil.harness_args(s) +
+    res = subprocess.run([exe, "render", ply, work, camf] + gpsutil.harness_args(s, taa_race_free=False) +
                          ["--checksum-only", "--time", "--warmup", str(args.warmup), "--dump-frames", "0",
                           "--no-post-dump"], capture_output=True, text=True, timeout=3000)
     if res.returncode != 0:

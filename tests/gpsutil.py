@@ -92,7 +92,7 @@ def write_camera_file(path: str, cams):
     rec.tofile(path)
 
 
-def harness_args(s) -> list[str]:
+def harness_args(s, taa_race_free: bool = True) -> list[str]:
     a = ["--res", str(s.width), str(s.height), "--ss", str(s.supersampling_factor), "--spp", str(s.samples_per_pixel),
          "--max-points", str(s.max_number_of_points), "--near", repr(float(s.near_view_plane)), "--far",
          repr(float(s.far_view_plane)), "--fovy", repr(float(s.fovy))]
@@ -115,7 +115,10 @@ def harness_args(s) -> list[str]:
     if s.immediate_splat_threshold > 0:
         a += ["--immediate-threshold", str(s.immediate_splat_threshold)]
     if s.accumulation_mode == gpsplat.GPS_ACCUM_TAA:
-        a.append("--taa")
+        # the harness runs the reference's own temporalRender so that no pixel reads a
+        # neighbour's blended value (its in-place blend otherwise races; see ref_harness.cu);
+        # timing runs keep the reference's own single launch
+        a.append("--taa-race-free" if taa_race_free else "--taa")
     elif s.accumulation_mode == gpsplat.GPS_ACCUM_NONE:
         a.append("--no-accumulation")
     return a

@@ -144,3 +144,21 @@ def test_oracle_splat_with_reference_workload(case):
     buf = o.buffer()
     agree = np.mean(buf == gold["f0_buffer"])
     assert agree > 0.99, f"splat buffer agrees at {agree:.5f} of entries"
+
+
+def test_host_cameras_match_the_library():
+    """The CPU baseline builds its settings and cameras without the CUDA library; they must
+    agree with the library's (gps_settings_default, gps_camera_from_pose) to float tolerance."""
+    import gpsplat
+    import synth
+
+    s_lib = gpsplat.default_settings(width=1920, height=1080, samples_per_pixel=4)
+    s_host = oracle.settings_host(width=1920, height=1080, samples_per_pixel=4)
+    assert bytes(s_lib) == bytes(s_host)
+    for p, r in synth.orbit(8, 30.0, 10.0) + synth.random_poses(8, seed=2):
+        lib = gpsplat.camera_to_numpy(gpsplat.camera_from_pose(p, np.asarray(r, np.float32).T, s_lib, 3))
+        host = gpsplat.camera_to_numpy(oracle.camera_host(p, r, s_host, 3))
+        for k in ("view", "proj", "position"):
+            np.testing.assert_allclose(host[k], lib[k], rtol=2e-5, atol=2e-4, err_msg=k)
+        # the far plane's offset (~1e4) cancels in single precision in the library
+        np.testing.assert_allclose(host["planes"], lib["planes"], rtol=5e-3, atol=2e-4, err_msg="planes")

@@ -69,6 +69,66 @@ def test_noalloc_scan_matches_renderer_twice(occlusion):
     scene.close()
 
 
+def _expected_scan(counts, bits, max_points):
+    """What the scan must produce, in numpy: survivors in Gaussian order, exclusive point
+    offsets mod 2^32, P = min(total, max_points) and each 256-point tile's first survivor."""
+    gid = np.nonzero(bits)[0].astype(np.uint32)
+    c = counts[gid].astype(np.uint64)
+    ex = np.concatenate([np.zeros(1, np.uint64), np.cumsum(c, dtype=np.uint64)[:-1]])
+    start = (ex & np.uint64(0xFFFFFFFF)).astype(np.uint32) if gid.size else np.zeros(0, np.uint32)
+    total = int(c.sum()) & 0xFFFFFFFF
+    points = min(total, max_points)
+    t = np.arange((points + 255) // 256, dtype=np.int64) * 256
+    owner = (np.searchsorted(start.astype(np.int64), t, side="right") - 1).astype(np.uint32)
+    return gid, start, total, points, int(total > max_points), owner
+
+
+def _run_exact_size(lib, counts, bits, max_points):
+    """Runs the scan on device buffers of exactly the documented sizes: counts up to n rounded
+    up to a multiple of 4, ceil(n / 32) mask words (with junk bits past n in the last word)."""
+    import torch
+
+    n = counts.size
+    c4 = np.zeros((n + 3) // 4 * 4, np.uint32)
+    c4[:n] = counts
+    words = np.zeros((n + 31) // 32 * 32, np.uint8)
+    words[:n] = bits
+    words[n:] = 1  # must be ignored
+    mask = np.packbits(words, bitorder="little").view(np.uint32)
+    d_counts = torch.from_numpy(c4.view(np.int32)).cuda()
+    d_mask = torch.from_numpy(mask.view(np.int32)).cuda()
+    gid = torch.full((n,), -1, dtype=torch.int32, device="cuda")
+    start = torch.full((n,), -1, dtype=torch.int32, device="cuda")
+    tiles = max_points // 256 + 2
+    tfr = torch.full((tiles,), -1, dtype=torch.int32, device="cuda")
+    ctr = torch.full((8,), -1, dtype=torch.int32, device="cuda")
+    st = lib.gps_workload_scan_noalloc(ctypes.c_void_p(d_counts.data_ptr()), ctypes.c_void_p(d_mask.data_ptr()), n,
+                                       max_points, ctypes.c_void_p(gid.data_ptr()), ctypes.c_void_p(start.data_ptr()),
+                                       ctypes.c_void_p(tfr.data_ptr()), ctypes.c_void_p(ctr.data_ptr()), None)
+    assert st == 0, lib.gps_last_error().decode()
+    torch.cuda.synchronize()
+    return (gid.cpu().numpy().view(np.uint32), start.cpu().numpy().view(np.uint32), tfr.cpu().numpy().view(np.uint32),
+            ctr.cpu().numpy().view(np.uint32))
+
+
+# odd sizes (partial last mask word, counts not a multiple of 16), and n = 2^25, the first size
+# that takes the scan's four-round tiles, with and without truncation
+@pytest.mark.parametrize("n,density,max_points", [(4097, 0.5, 10**6), (60001, 0.3, 10**6), (60001, 0.9, 50000),
+                                                  (33554432, 0.3, 250_000_000), (33554432, 0.3, 40_000_000)])
+def test_noalloc_scan_matches_numpy(n, density, max_points):
+    lib = gpsplat.load_library()
+    rng = np.random.default_rng(n ^ int(density * 100) ^ max_points)
+    counts = rng.integers(0, 21, n, dtype=np.uint32)
+    bits = rng.random(n) < density
+    gid_w, start_w, total, points, trunc, owner_w = _expected_scan(counts, bits, max_points)
+    for call in range(2):
+        gid, start, tfr, c = _run_exact_size(lib, counts, bits, max_points)
+        assert c[0] == gid_w.size and c[1] == total and c[2] == points and c[3] == trunc, f"call {call}: counters {c[:4]}"
+        assert np.array_equal(gid[: gid_w.size], gid_w), f"call {call}: survivor ids differ"
+        assert np.array_equal(start[: gid_w.size], start_w), f"call {call}: first points differ"
+        assert np.array_equal(tfr[: owner_w.size], owner_w), f"call {call}: tile owners differ"
+
+
 def test_noalloc_scan_rejects_oversized_input():
     lib = gpsplat.load_library()
     # null buffers: the size check answers first, and the null check would stop the call
