@@ -158,6 +158,52 @@ GPS_HD mat3 quat_to_rotmat(vec4 q) {
 }
 
 // linalg.cuh:324-342: Sigma = (R S)(R S)^T with S = diag(scale)
+#if defined(__CUDA_ARCH__)
+// On the device the 3D covariance is spelled out with round-to-nearest intrinsics, which the
+// compiler never contracts or reorders, in the rounding pattern of the reference's compiled
+// quaternion-to-matrix and M * M^T (glm's mat3_cast and mat3 product): which products are
+// rounded on their own and which are fused into the following add.  Left to the compiler, the
+// same expressions contract differently inside different kernels; in the preprocess that gave
+// 1-ulp different off-diagonal terms for about a third of the Gaussians, hence 1-ulp different
+// sample positions.  The pattern was fitted against the reference's own kernels (bit-identical
+// covariances for every survivor of a 2M-Gaussian town frame, up to the sign of exact zeros,
+// which fast-math code does not preserve).
+GPS_D mat3 scale_rot_to_cov(vec3 scale, vec4 quat) {
+    const float w = quat.x, x = quat.y, y = quat.z, z = quat.w;
+    const float qxx = __fmul_rn(x, x), qyy = __fmul_rn(y, y), qzz = __fmul_rn(z, z);
+    const float qxz = __fmul_rn(x, z), qxy = __fmul_rn(x, y), qyz = __fmul_rn(y, z);
+    const float qwx = __fmul_rn(w, x), qwy = __fmul_rn(w, y), qwz = __fmul_rn(w, z);
+    (void)qxx;
+    mat3 r;  // columns, as glm::toMat3
+    r.c[0].x = __fsub_rn(1.0f, __fmul_rn(2.0f, __fadd_rn(qyy, qzz)));
+    r.c[0].y = __fmul_rn(2.0f, __fmaf_rn(x, y, qwz));
+    r.c[0].z = __fmul_rn(2.0f, __fmaf_rn(x, z, -qwy));
+    r.c[1].x = __fmul_rn(2.0f, __fmaf_rn(x, y, -qwz));
+    r.c[1].y = __fsub_rn(1.0f, __fmul_rn(2.0f, __fmaf_rn(x, x, qzz)));
+    r.c[1].z = __fmul_rn(2.0f, __fmaf_rn(w, x, qyz));
+    r.c[2].x = __fmul_rn(2.0f, __fmaf_rn(x, z, qwy));
+    r.c[2].y = __fmul_rn(2.0f, __fmaf_rn(-w, x, qyz));
+    r.c[2].z = __fsub_rn(1.0f, __fmul_rn(2.0f, __fmaf_rn(x, x, qyy)));
+    const float sc[3] = {scale.x, scale.y, scale.z};
+    float m[3][3];  // m[k][i] = M column k, row i = R column k, row i * scale_k
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        m[k][0] = __fmul_rn(r.c[k].x, sc[k]);
+        m[k][1] = __fmul_rn(r.c[k].y, sc[k]);
+        m[k][2] = __fmul_rn(r.c[k].z, sc[k]);
+    }
+    // (M M^T)[c][i] = (M[0][i] M[0][c] + M[1][i] M[1][c]) + M[2][i] M[2][c]: the middle product
+    // rounded, the first and last fused
+    auto el = [&](int c, int i) {
+        return __fmaf_rn(m[2][i], m[2][c], __fmaf_rn(m[0][i], m[0][c], __fmul_rn(m[1][i], m[1][c])));
+    };
+    mat3 out;
+    out.c[0] = make_v3(el(0, 0), el(0, 1), el(0, 2));
+    out.c[1] = make_v3(out.c[0].y, el(1, 1), el(1, 2));
+    out.c[2] = make_v3(out.c[0].z, out.c[1].z, el(2, 2));
+    return out;
+}
+#else
 GPS_HD mat3 scale_rot_to_cov(vec3 scale, vec4 quat) {
     mat3 r = quat_to_rotmat(quat);
     mat3 s = mat3_identity(1.0f);
@@ -167,6 +213,7 @@ GPS_HD mat3 scale_rot_to_cov(vec3 scale, vec4 quat) {
     mat3 m = r * s;
     return m * transpose(m);
 }
+#endif
 
 // linalg.cuh:221-249: EWA projection of the 3D covariance (Zwicker et al. 2002, eq. 29/31),
 // returns (cov[0][0], cov[0][1], cov[1][1]).

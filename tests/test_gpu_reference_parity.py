@@ -166,3 +166,56 @@ def test_reference_parity(case):
     if case in GROUPED_MIN_POINTS and grouped_frames == 0:
         problems.append(f"no frame had >= {GROUPED_MIN_POINTS[case]} points in every pass: the grouped walk was not covered")
     assert not problems, "\n".join(problems)
+
+
+def test_record_geometry_matches_reference_projection():
+    """Every survivor's splat record against the reference's own loadAndTransformGaussian
+    (gaussian_point_splatting.cu:17-65, run by the harness's probe mode on the same PLY and
+    camera): pixel mean, tile bounds and c0 = sqrt(cov2d.x) bit for bit.  A one-ulp slip in the
+    2D covariance moves only the rare samples that sit on a pixel edge, so the splat-buffer
+    comparison alone catches it only on large scenes; this compares the values themselves."""
+    import os
+    import subprocess
+    import tempfile
+
+    exe = gpsutil.ref_harness("fp32")
+    if exe is None:
+        pytest.skip("reference harness not built (oracle/ref/build_ref.sh)")
+    ply = gpsutil.cached_ply("town60k", lambda: synth.town(60000, seed=5))
+    s = gpsplat.default_settings(width=1920, height=1080, supersampling_factor=2, samples_per_pixel=1,
+                                 enable_occlusion_culling=0)
+    cams = gpsutil.cameras_for(s, synth.orbit(3, 30.0, 10.0))
+    scene = gpsplat.Scene.from_ply(ply, gpsplat.GPS_SCENE_FP32)
+    n = scene.count
+    u = lambda a: np.ascontiguousarray(a, np.float32).view(np.uint32)
+    for cam in cams:
+        r = gpsplat.Renderer(scene, s)
+        loop = gpsplat.FrameLoop(r)
+        loop.step(cam)
+        gpsutil.sync()
+        v = r.debug_view()
+        mask = gpsutil.mask_bits(gpsutil.d2h(v.mask_last, (n + 31) // 32, np.uint32), n)
+        ids = np.nonzero(mask)[0].astype(np.uint32)
+        rec = gpsutil.d2h(v.records, n * 16, np.float32).reshape(n, 16)[ids]
+        loop.close()
+        r.close()
+        assert ids.size > 1000
+        work = tempfile.mkdtemp(prefix="gps_probe_")
+        camf = os.path.join(work, "cams.bin")
+        gpsutil.write_camera_file(camf, [cam])
+        ids.tofile(os.path.join(work, "ids.u32"))
+        res = subprocess.run([exe, "probe", ply, work, camf, os.path.join(work, "ids.u32"), "--res", str(s.width),
+                              str(s.height), "--ss", str(s.supersampling_factor)], capture_output=True, text=True,
+                             timeout=600)
+        assert res.returncode == 0, res.stderr[-1000:]
+        pr = np.load(os.path.join(work, "probe.npy"))
+        assert (pr[:, 47] == 1.0).all(), "the reference culls a Gaussian this library kept"
+        assert np.array_equal(u(rec[:, 0:2]), u(pr[:, 29:31])), "pixel means differ"
+        c0_ref = np.sqrt(pr[:, 25].astype(np.float32))  # IEEE sqrt, as __fsqrt_rn
+        bad = np.nonzero(u(rec[:, 2]) != u(c0_ref))[0]
+        assert bad.size == 0, f"frame {cam.frame}: c0 differs for {bad.size} of {ids.size} survivors"
+        bounds = rec[:, 12:14].view(np.uint32)
+        mn = np.stack([bounds[:, 0] & 0xFFFF, bounds[:, 0] >> 16], axis=1).astype(np.float32)
+        mx = np.stack([bounds[:, 1] & 0xFFFF, bounds[:, 1] >> 16], axis=1).astype(np.float32)
+        assert np.array_equal(mn, pr[:, 31:33]) and np.array_equal(mx, pr[:, 33:35]), "tile bounds differ"
+    scene.close()
