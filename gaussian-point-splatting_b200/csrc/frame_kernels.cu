@@ -182,11 +182,14 @@ __device__ __forceinline__ void splat_samples_unbiased(u32x2& seed, const SplatR
 // gaussian_point_splatting.cu:272-287), and it is no survivor.
 template <class Scene, bool kImmediate>
 __device__ __forceinline__ bool preprocess_one(const PreprocessArgs& a, const Scene& scene, uint32_t gi,
-                                               const uint32_t* __restrict__ mask_prev, bool& loaded) {
+                                               const uint32_t* __restrict__ mask_prev, bool& loaded,
+                                               uint32_t& out_points, uint32_t& out_bin) {
     const int idx = (int)gi;
     const FrameConst& fc = a.fc;
     bool splats = false;
     loaded = false;
+    out_points = 0;
+    out_bin = 0xFFFFFFFFu;
     do {
         if (idx >= (int)a.n) break;
         if (fc.enable_hier && block_culled(a.blocks, (uint32_t)idx)) break;
@@ -290,6 +293,9 @@ __device__ __forceinline__ bool preprocess_one(const PreprocessArgs& a, const Sc
         }
         a.records[idx] = rec;
         a.counts[idx] = num_points;
+        out_points = num_points;
+        if (a.bins)
+            out_bin = screen_bin(pixel_mean.x, pixel_mean.y, fc.up_width, fc.up_height, a.bin_shift, a.bins_x, a.bins_y);
         splats = true;
     } while (false);
     return splats;
@@ -311,20 +317,64 @@ __global__ void __launch_bounds__(256) preprocess_kernel(PreprocessArgs a, Scene
     const uint32_t warps = gridDim.x * (blockDim.x >> 5);
     const uint32_t first = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
     uint32_t loaded_tally = 0;  // this warp's Gaussians whose attributes were read
+    // this warp's running survivor / point totals of one scan tile, flushed on a tile change
+    uint32_t tile = 0xFFFFFFFFu, tile_s = 0, tile_p = 0;
+    auto flush_tile = [&]() {
+        if (lane == 0 && tile != 0xFFFFFFFFu && tile_s) {
+            // two 32-bit halves: the point total wraps mod 2^32 without carrying into the count
+            uint32_t* w = reinterpret_cast<uint32_t*>(a.tile_totals + tile);
+            atomicAdd(w, tile_p);
+            atomicAdd(w + 1, tile_s);
+        }
+    };
     auto chunk = [&](uint32_t c) {
         bool loaded;
-        const bool splats = preprocess_one<Scene, kImmediate>(a, scene, (c << 5) + lane, mask_prev, loaded);
+        uint32_t pts, bin;
+        const bool splats = preprocess_one<Scene, kImmediate>(a, scene, (c << 5) + lane, mask_prev, loaded, pts, bin);
         const unsigned m = __ballot_sync(0xffffffffu, splats);
         loaded_tally += (uint32_t)__popc(__ballot_sync(0xffffffffu, loaded));
         if (lane == 0) mask_cur[c] = m;
+        if (a.tile_totals && m) {
+            const uint32_t t = (c << 5) >> a.tile_shift;
+            if (t != tile) {
+                flush_tile();
+                tile = t;
+                tile_s = tile_p = 0;
+            }
+            tile_s += (uint32_t)__popc(m);
+            tile_p += __reduce_add_sync(0xffffffffu, pts);
+        }
+        if (a.bins && m) {  // one atomic per distinct bin among the warp's survivors
+            unsigned todo = m;
+            while (todo) {
+                const uint32_t key = __shfl_sync(0xffffffffu, bin, __ffs(todo) - 1);
+                const unsigned members = __ballot_sync(0xffffffffu, ((todo >> lane) & 1u) && bin == key);
+                const uint32_t sum = __reduce_add_sync(0xffffffffu, ((members >> lane) & 1u) ? pts : 0u);
+                if (lane == 0) atomicAdd(a.bins + key, ((unsigned long long)__popc(members) << 32) | sum);
+                todo &= ~members;
+            }
+        }
     };
     if (a.chunk_list) {
         const uint32_t count = *a.chunk_count;
-        for (uint32_t i = first; i < count; i += warps) chunk(__ldg(a.chunk_list + i));
+        if (a.tile_totals) {  // contiguous ranges of the (ascending) list, so tile totals merge
+            const uint32_t per = (count + warps - 1) / warps;
+            const uint32_t b = first * per, e = min(count, b + per);
+            for (uint32_t i = b; i < e; ++i) chunk(__ldg(a.chunk_list + i));
+        } else {
+            for (uint32_t i = first; i < count; i += warps) chunk(__ldg(a.chunk_list + i));
+        }
     } else {
         const uint32_t chunks = (a.n + 31u) >> 5;
-        for (uint32_t c = first; c < chunks; c += warps) chunk(c);
+        if (a.tile_totals) {
+            const uint32_t per = (chunks + warps - 1) / warps;
+            const uint32_t b = first * per, e = min(chunks, b + per);
+            for (uint32_t c = b; c < e; ++c) chunk(c);
+        } else {
+            for (uint32_t c = first; c < chunks; c += warps) chunk(c);
+        }
     }
+    flush_tile();
     if (a.loaded && lane == 0 && loaded_tally) atomicAdd(a.loaded, loaded_tally);
 }
 
@@ -419,13 +469,17 @@ __global__ void __launch_bounds__(kScanThreads) scan_reduce_kernel(ScanArgs a) {
 // each thread scans 4 consecutive words and a block scan plus a running carry joins them.
 constexpr int kTileScanThreads = 1024;
 constexpr int kTileScanPer = 4;
-__global__ void __launch_bounds__(kTileScanThreads) scan_tiles_kernel(ScanArgs a, uint32_t num_tiles) {
+
+// One block: exclusive prefix of `count` packed (survivors << 32 | points) words in place,
+// through shared memory in coalesced rounds; returns the totals.
+__device__ __forceinline__ void scan_words_inplace(unsigned long long* words_g, uint32_t count, uint32_t& total_s,
+                                                   uint32_t& total_p) {
     __shared__ unsigned long long words[kTileScanThreads * kTileScanPer];
     constexpr uint32_t kRound = kTileScanThreads * kTileScanPer;
     uint32_t carry_s = 0, carry_p = 0;
-    for (uint32_t r0 = 0; r0 < num_tiles; r0 += kRound) {
+    for (uint32_t r0 = 0; r0 < count; r0 += kRound) {
         for (uint32_t i = threadIdx.x; i < kRound; i += kTileScanThreads)
-            words[i] = r0 + i < num_tiles ? a.tile_state[r0 + i] : 0ull;
+            words[i] = r0 + i < count ? words_g[r0 + i] : 0ull;
         __syncthreads();
         uint32_t s = 0, p = 0;
 #pragma unroll
@@ -446,11 +500,25 @@ __global__ void __launch_bounds__(kTileScanThreads) scan_tiles_kernel(ScanArgs a
             ex_p += (uint32_t)v;
         }
         __syncthreads();
-        for (uint32_t i = threadIdx.x; i < kRound && r0 + i < num_tiles; i += kTileScanThreads) a.tile_state[r0 + i] = words[i];
+        for (uint32_t i = threadIdx.x; i < kRound && r0 + i < count; i += kTileScanThreads) words_g[r0 + i] = words[i];
         carry_s += tot_s;
         carry_p += tot_p;
         __syncthreads();
     }
+    total_s = carry_s;
+    total_p = carry_p;
+}
+
+// Pass 2: block 0 turns the tile totals into exclusive tile prefixes (in place) and writes the
+// pass counters (points mod 2^32, like the reference's u32 offsets); block 1, when the pass is
+// screen-binned, does the same for the bin histogram.
+__global__ void __launch_bounds__(kTileScanThreads) scan_tiles_kernel(ScanArgs a, uint32_t num_tiles) {
+    uint32_t carry_s, carry_p;
+    if (blockIdx.x == 1) {
+        scan_words_inplace(a.bins, a.nbins, carry_s, carry_p);
+        return;
+    }
+    scan_words_inplace(a.tile_state, num_tiles, carry_s, carry_p);
     if (threadIdx.x == 0) {
         a.counters->survivors = carry_s;
         a.counters->total_points = carry_p;
@@ -501,23 +569,82 @@ __global__ void __launch_bounds__(kScanThreads) scan_write_kernel(ScanArgs a) {
     }
 }
 
+// The render path's downsweep: as scan_write_kernel, and then for every survivor the splat's
+// work order.  Screen-binned (bins set, pass not truncated): the survivor takes its slot and
+// first walk position from its bin's cursor with one 64-bit atomic, so that slot and position
+// stay consistent and positions increase with the slot; otherwise the Gaussian order itself,
+// with the points past P dropped as the reference drops them.  Either way the survivor then
+// records itself as the owner of every 256-point splat tile that starts inside its points.
+// (tiles starting at or past P are never walked, and the array holds max_points / 256 + 2)
+__device__ __forceinline__ void own_tiles(uint32_t* __restrict__ tile_first_rank, uint64_t first, uint64_t count,
+                                          uint32_t rank, uint32_t P) {
+    const uint64_t end = min(first + count, (uint64_t)P);
+    for (uint64_t t = (first + 255u) >> 8; (t << 8) < end; ++t) tile_first_rank[t] = rank;
+}
+
+template <int kScanRounds>
+__global__ void __launch_bounds__(kScanThreads) scan_write_fused_kernel(ScanArgs a) {
+    const uint32_t* mask = a.mask;
+    if (a.mask_iter) mask = (*a.mask_iter & 1u) ? a.mask_pair[1] : a.mask_pair[0];
+    const uint32_t tile = blockIdx.x;
+    const uint32_t base = tile * (kScanThreads * kScanItems * kScanRounds) + threadIdx.x * (kScanItems * kScanRounds);
+    uint32_t surv = 0, pts = 0;
+#pragma unroll
+    for (int q = 0; q < kScanRounds; ++q) {
+        uint32_t cnt[kScanItems];
+        surv += __popc(scan_load(a, mask, base + q * kScanItems, cnt));
+#pragma unroll
+        for (int i = 0; i < kScanItems; ++i) pts += cnt[i];
+    }
+    uint32_t ex_s, ex_p, tot_s, tot_p;
+    block_scan_pair<kScanThreads>(surv, pts, ex_s, ex_p, tot_s, tot_p);
+    if (surv == 0u) return;
+    const uint32_t P = a.counters->points;
+    const bool binned = a.bins && a.counters->truncated == 0u;
+    const unsigned long long pre = a.tile_state[tile];
+    uint32_t r = (uint32_t)(pre >> 32) + ex_s;
+    uint32_t pt = (uint32_t)pre + ex_p;
+    for (int q = 0; q < kScanRounds; ++q) {  // again, now writing (the counts come from L1/L2)
+        uint32_t cnt[kScanItems];
+        const uint32_t b = base + q * kScanItems;
+        const uint32_t bits = scan_load(a, mask, b, cnt);
+#pragma unroll
+        for (int i = 0; i < kScanItems; ++i) {
+            if ((bits >> i) & 1u) {
+                const uint32_t g = b + i;
+                a.surv_gid[r] = g;
+                a.surv_start[r] = pt;
+                if (binned) {
+                    const float2 pm = __ldg(reinterpret_cast<const float2*>(a.records + g));
+                    const uint32_t bin = screen_bin(pm.x, pm.y, a.up_width, a.up_height, a.bin_shift, a.bins_x, a.bins_y);
+                    const unsigned long long old = atomicAdd(a.bins + bin, (1ull << 32) | cnt[i]);
+                    const uint32_t slot = (uint32_t)(old >> 32);
+                    a.sorted_gid[slot] = g;
+                    a.sorted_pstart[slot] = pt;
+                    a.sorted_qstart[slot] = (uint32_t)old;
+                    own_tiles(a.tile_first_rank, (uint32_t)old, cnt[i], slot, P);
+                } else if (pt < P) {
+                    own_tiles(a.tile_first_rank, pt, cnt[i], r, P);
+                }
+                ++r;
+                pt += cnt[i];
+            }
+        }
+    }
+}
+
 // First survivor of every splat tile: tile t (points [t*tile_points, ...)) starts inside the
 // survivor with the largest rank whose first point is <= t*tile_points.  One thread per tile,
 // a binary search over the survivors' first points (monotone below 2^32 points per pass).  A
 // survivor can own thousands of tiles (a Gaussian right in front of the camera), so this is
 // done per tile rather than per survivor.
-// With `bins` set the survivors are in screen-bin order: their count is the binned one
-// (counters->pad[0]) and the bin cursors are cleared here for the next pass.
 __global__ void __launch_bounds__(256) tile_owner_kernel(const uint32_t* __restrict__ surv_start,
                                                          uint32_t* __restrict__ tile_first_rank,
                                                          const PassCounters* __restrict__ counters,
-                                                         uint32_t tile_points, uint32_t* __restrict__ mask_iter,
-                                                         unsigned long long* __restrict__ bins, uint32_t nbins) {
+                                                         uint32_t tile_points, uint32_t* __restrict__ mask_iter) {
     const uint32_t points = counters->points;
-    const uint32_t survivors = bins ? counters->pad[0] : counters->survivors;
+    const uint32_t survivors = counters->survivors;
     if (mask_iter && points > 0 && blockIdx.x == 0 && threadIdx.x == 0) *mask_iter += 1u;
-    if (bins)
-        for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i <= nbins; i += gridDim.x * blockDim.x) bins[i] = 0ull;
     if (points == 0 || survivors == 0) return;
     const uint32_t tiles = (uint32_t)(((unsigned long long)points + tile_points - 1) / tile_points);
     for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < tiles; t += gridDim.x * blockDim.x) {
@@ -529,87 +656,6 @@ __global__ void __launch_bounds__(256) tile_owner_kernel(const uint32_t* __restr
             else hi = mid - 1;
         }
         tile_first_rank[t] = lo;
-    }
-}
-
-// ---------------------------------------------------------------------------------
-// Screen-tile binning of a pass's survivors (BinArgs): a histogram of (survivors, points) per
-// bin, an in-place exclusive scan of the bins, then a scatter in which each survivor takes its
-// slot and first walk position from its bin's cursor with one 64-bit atomic (so the two stay
-// consistent and the walk positions increase with the slot).  Points past P are dropped here,
-// as the reference drops them.
-// ---------------------------------------------------------------------------------
-__device__ __forceinline__ bool survivor_bin(const BinArgs& a, uint32_t r, uint32_t points, uint32_t& g,
-                                             uint32_t& start, uint32_t& eff, uint32_t& bin) {
-    g = __ldg(a.surv_gid + r);
-    start = __ldg(a.surv_start + r);
-    if (start >= points) return false;
-    eff = min(__ldg(a.counts + g), points - start);
-    if (eff == 0u) return false;
-    const float2 pm = __ldg(reinterpret_cast<const float2*>(a.records + g));
-    const float x = fminf(fmaxf(pm.x, 0.0f), (float)(a.up_width - 1));   // NaN -> 0
-    const float y = fminf(fmaxf(pm.y, 0.0f), (float)(a.up_height - 1));
-    const int bx = min((int)x >> a.bin_shift, a.bins_x - 1);
-    const int by = min((int)y >> a.bin_shift, a.bins_y - 1);
-    bin = (uint32_t)(by * a.bins_x + bx);
-    return true;
-}
-
-__global__ void __launch_bounds__(256) bin_count_kernel(BinArgs a) {
-    const uint32_t survivors = a.counters->survivors, points = a.counters->points;
-    for (uint32_t r = blockIdx.x * blockDim.x + threadIdx.x; r < survivors; r += gridDim.x * blockDim.x) {
-        uint32_t g, start, eff, bin;
-        if (survivor_bin(a, r, points, g, start, eff, bin)) atomicAdd(a.bins + bin, (1ull << 32) | eff);
-    }
-}
-
-// One block: exclusive prefix of the bin words in place (rounds through shared memory, as in
-// scan_tiles_kernel); the binned survivor count goes to counters->pad[0].
-__global__ void __launch_bounds__(kTileScanThreads) bin_scan_kernel(BinArgs a) {
-    __shared__ unsigned long long words[kTileScanThreads * kTileScanPer];
-    constexpr uint32_t kRound = kTileScanThreads * kTileScanPer;
-    uint32_t carry_s = 0, carry_p = 0;
-    for (uint32_t r0 = 0; r0 < a.nbins; r0 += kRound) {
-        for (uint32_t i = threadIdx.x; i < kRound; i += kTileScanThreads)
-            words[i] = r0 + i < a.nbins ? a.bins[r0 + i] : 0ull;
-        __syncthreads();
-        uint32_t sv = 0, pt = 0;
-#pragma unroll
-        for (int k = 0; k < kTileScanPer; ++k) {
-            const unsigned long long v = words[threadIdx.x * kTileScanPer + k];
-            sv += (uint32_t)(v >> 32);
-            pt += (uint32_t)v;
-        }
-        uint32_t ex_s, ex_p, tot_s, tot_p;
-        block_scan_pair<kTileScanThreads>(sv, pt, ex_s, ex_p, tot_s, tot_p);
-        ex_s += carry_s;
-        ex_p += carry_p;
-#pragma unroll
-        for (int k = 0; k < kTileScanPer; ++k) {
-            const unsigned long long v = words[threadIdx.x * kTileScanPer + k];
-            words[threadIdx.x * kTileScanPer + k] = ((unsigned long long)ex_s << 32) | ex_p;
-            ex_s += (uint32_t)(v >> 32);
-            ex_p += (uint32_t)v;
-        }
-        __syncthreads();
-        for (uint32_t i = threadIdx.x; i < kRound && r0 + i < a.nbins; i += kTileScanThreads) a.bins[r0 + i] = words[i];
-        carry_s += tot_s;
-        carry_p += tot_p;
-        __syncthreads();
-    }
-    if (threadIdx.x == 0) a.counters->pad[0] = carry_s;
-}
-
-__global__ void __launch_bounds__(256) bin_scatter_kernel(BinArgs a) {
-    const uint32_t survivors = a.counters->survivors, points = a.counters->points;
-    for (uint32_t r = blockIdx.x * blockDim.x + threadIdx.x; r < survivors; r += gridDim.x * blockDim.x) {
-        uint32_t g, start, eff, bin;
-        if (!survivor_bin(a, r, points, g, start, eff, bin)) continue;
-        const unsigned long long old = atomicAdd(a.bins + bin, (1ull << 32) | eff);
-        const uint32_t slot = (uint32_t)(old >> 32);
-        a.sorted_gid[slot] = g;
-        a.sorted_pstart[slot] = start;
-        a.sorted_qstart[slot] = (uint32_t)old;
     }
 }
 
@@ -904,12 +950,26 @@ constexpr int kSplatWindow = kSplatTile * kSplatRounds;
 
 // K > 0: unbiased splatting with K points per thread per pass; K = 0: any other setting.
 template <int K>
-__global__ void __launch_bounds__(kSplatTile, kSplatRounds > 1 ? 4 : 1) splat_kernel(SplatArgs a) {
+#ifndef GPS_SPLAT_MIN_BLOCKS
+#define GPS_SPLAT_MIN_BLOCKS 4
+#endif
+__global__ void __launch_bounds__(kSplatTile, kSplatRounds > 1 ? GPS_SPLAT_MIN_BLOCKS : 1) splat_kernel(SplatArgs a) {
     __shared__ uint32_t s_start[kSplatWindow];
     __shared__ uint32_t s_spread[kTileSize];
     if (GPS_SPLAT_MORTON_LUT && threadIdx.x < kTileSize) s_spread[threadIdx.x] = morton_spread(threadIdx.x);
     const uint32_t points = a.counters->points;
-    const uint32_t survivors = a.point_base ? a.counters->pad[0] : a.counters->survivors;
+    const uint32_t survivors = a.counters->survivors;
+    // the pass's work order: screen bins unless the scan had to truncate the pass
+    const bool binned = a.sorted_gid && a.counters->truncated == 0u;
+    const uint32_t* __restrict__ gids = binned ? a.sorted_gid : a.surv_gid;
+    const uint32_t* __restrict__ first_q = binned ? a.sorted_qstart : a.surv_start;
+    const uint32_t* __restrict__ point_base = binned ? a.sorted_pstart : nullptr;
+    // the preprocess of the next pass accumulates into these; nothing here reads them
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < a.clear_a_words; i += gridDim.x * blockDim.x)
+        a.clear_a[i] = 0ull;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < a.clear_b_words; i += gridDim.x * blockDim.x)
+        a.clear_b[i] = 0ull;
+    if (a.mask_iter && points > 0u && blockIdx.x == 0 && threadIdx.x == 0) *a.mask_iter += 1u;
     // splats walk position q0 + threadIdx.x of a tile whose survivor starts are in `starts`
     auto splat_tile_point = [&](uint32_t q0, uint32_t r0, const uint32_t* starts, int window) {
         const uint32_t q = q0 + threadIdx.x;
@@ -922,8 +982,8 @@ __global__ void __launch_bounds__(kSplatTile, kSplatRounds > 1 ? 4 : 1) splat_ke
             }
             // the reference's point index (the seed): the walk position itself in Gaussian
             // order, the survivor's first point plus the offset in screen-bin order
-            const uint32_t p = a.point_base ? __ldg(&a.point_base[r0 + lo]) + (q - starts[lo]) : q;
-            const uint32_t g = __ldg(&a.surv_gid[r0 + lo]);
+            const uint32_t p = point_base ? __ldg(&point_base[r0 + lo]) + (q - starts[lo]) : q;
+            const uint32_t g = __ldg(&gids[r0 + lo]);
             if (g < a.n) {  // always true unless the scan gave up (device_timeouts)
                 const float4* rp = reinterpret_cast<const float4*>(a.records + g);
                 SplatRecord rec;
@@ -942,7 +1002,7 @@ __global__ void __launch_bounds__(kSplatTile, kSplatRounds > 1 ? 4 : 1) splat_ke
     };
     auto start_of = [&](uint32_t r0, uint32_t k) {
         const uint32_t r = r0 + k;
-        return (r0 < survivors && r < survivors) ? a.surv_start[r] : 0xFFFFFFFFu;
+        return (r0 < survivors && r < survivors) ? first_q[r] : 0xFFFFFFFFu;
     };
     // grouped tiles only while there are at least two groups per block; a small pass keeps one
     // tile per barrier so that its points still spread over every block
@@ -1537,7 +1597,21 @@ static_assert(kScanTile == kScanTileGaussians, "scan tile size");
 // tile words a scan of n Gaussians may use (the small-tile count, an upper bound)
 uint32_t scan_tile_count(uint32_t n) { return (uint32_t)(((uint64_t)n + kScanTileSmall - 1) / kScanTileSmall); }
 
-void launch_scan(const ScanArgs& a, uint32_t scan_tiles, cudaStream_t stream, bool owners) {
+int scan_tile_shift(uint32_t n) { return n >= kScanBigScene ? 14 : 12; }
+
+void launch_scan_fused(const ScanArgs& a, cudaStream_t stream) {
+    if (a.n == 0) {
+        cudaMemsetAsync(a.counters, 0, sizeof(PassCounters), stream);
+        return;
+    }
+    const bool big = a.n >= kScanBigScene;
+    const uint32_t tiles = (uint32_t)(((uint64_t)a.n + (big ? kScanTile : kScanTileSmall) - 1) / (big ? kScanTile : kScanTileSmall));
+    launch_k(scan_tiles_kernel, a.bins ? 2 : 1, kTileScanThreads, 0, stream, a, tiles);
+    if (big) launch_k(scan_write_fused_kernel<kScanRoundsMax>, tiles, kScanThreads, 0, stream, a);
+    else launch_k(scan_write_fused_kernel<1>, tiles, kScanThreads, 0, stream, a);
+}
+
+void launch_scan(const ScanArgs& a, uint32_t scan_tiles, cudaStream_t stream) {
     if (scan_tiles == 0 || a.n == 0) {
         cudaMemsetAsync(a.counters, 0, sizeof(PassCounters), stream);
         return;
@@ -1556,21 +1630,8 @@ void launch_scan(const ScanArgs& a, uint32_t scan_tiles, cudaStream_t stream, bo
     const uint64_t max_tiles = ((uint64_t)a.max_points + a.tile_points - 1) / a.tile_points;
     const uint64_t want = (max_tiles + 255) / 256;
     const int owner_grid = (int)(want < 1184 ? (want ? want : 1) : 1184);  // 148 SMs x 8
-    if (owners)
-        launch_k(tile_owner_kernel, owner_grid, 256, 0, stream, a.surv_start, a.tile_first_rank, a.counters,
-                 a.tile_points, a.mask_iter, (unsigned long long*)nullptr, 0u);
-}
-
-void launch_bin(const BinArgs& b, const ScanArgs& a, cudaStream_t stream) {
-    const int grid = 148 * 8;
-    launch_k(bin_count_kernel, grid, 256, 0, stream, b);
-    launch_k(bin_scan_kernel, 1, kTileScanThreads, 0, stream, b);
-    launch_k(bin_scatter_kernel, grid, 256, 0, stream, b);
-    const uint64_t max_tiles = ((uint64_t)a.max_points + a.tile_points - 1) / a.tile_points;
-    const uint64_t want = (max_tiles + 255) / 256;
-    const int owner_grid = (int)std::max<uint64_t>(1, std::min<uint64_t>(want, 148 * 8));
-    launch_k(tile_owner_kernel, owner_grid, 256, 0, stream, (const uint32_t*)b.sorted_qstart, a.tile_first_rank,
-             (const PassCounters*)b.counters, a.tile_points, a.mask_iter, b.bins, b.nbins);
+    launch_k(tile_owner_kernel, owner_grid, 256, 0, stream, a.surv_start, a.tile_first_rank, a.counters, a.tile_points,
+             a.mask_iter);
 }
 
 template <int K>

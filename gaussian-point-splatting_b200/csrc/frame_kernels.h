@@ -89,6 +89,13 @@ struct PreprocessArgs {
     uint32_t* mask_pair[2];
     const uint32_t* mask_iter;
     uint32_t* loaded;             // tally of Gaussians whose attributes were read (null: none)
+    // Pass workload accumulated here (render path; null: not accumulated): per scan tile of
+    // 2^tile_shift Gaussians, survivors in the high and points (mod 2^32) in the low word; per
+    // screen bin, survivors << 32 | points.  Both are zero on entry.
+    unsigned long long* tile_totals;
+    int tile_shift;
+    unsigned long long* bins;
+    int bin_shift, bins_x, bins_y;
 };
 
 struct ScanArgs {
@@ -109,46 +116,55 @@ struct ScanArgs {
     unsigned long long* tile_state;  // [scan tiles] tile totals, then tile prefixes
     PassCounters* counters;
     uint32_t* loaded;            // the preprocess's tally: moved into counters->loaded and reset
+    // Screen binning in the downsweep (render path; null bins: Gaussian order): the bin scan runs
+    // beside the tile scan, and the downsweep scatters the survivors into bin order
+    unsigned long long* bins;
+    uint32_t nbins;
+    int bin_shift, bins_x, bins_y, up_width, up_height;
+    const SplatRecord* records;
+    uint32_t* sorted_gid;        // [n] survivors in bin order
+    uint32_t* sorted_pstart;     //     their first points (reference point indices)
+    uint32_t* sorted_qstart;     //     their first walk positions in bin order
 };
 
 struct SplatArgs {
     FrameConst fc;
     int frame_seed;
     const SplatRecord* records;
-    const uint32_t* surv_gid;
-    const uint32_t* surv_start;      // first walk position of each survivor (monotone)
+    const uint32_t* surv_gid;        // survivors in Gaussian order: a walk position is a point index
+    const uint32_t* surv_start;      // first point of each survivor (monotone)
     const uint32_t* tile_first_rank;
     const PassCounters* counters;
     uint64_t* buffer;
     uint32_t n;
-    // Screen-binned order (null: Gaussian order, where a walk position is the point index):
-    // survivor i's points are the reference's point indices point_base[i] + (q - surv_start[i]).
-    const uint32_t* point_base;
+    // Screen-binned order (null sorted_gid, or a truncated pass: Gaussian order): survivor i's
+    // points are the reference's point indices sorted_pstart[i] + (q - sorted_qstart[i]).
+    const uint32_t* sorted_gid;
+    const uint32_t* sorted_qstart;
+    const uint32_t* sorted_pstart;
+    // cleared for the next pass once this pass's workload is consumed (null: nothing)
+    unsigned long long* clear_a;
+    uint32_t clear_a_words;
+    unsigned long long* clear_b;
+    uint32_t clear_b_words;
+    uint32_t* mask_iter;             // advanced after a pass with points (null: not here)
 };
 
-// Screen-tile binning of one pass's survivors: the splat walks survivors grouped by the 64x64
-// splat-buffer tile (or block of tiles) holding their pixel mean, so that blocks running at the
-// same time write a compact part of the buffer.  Only the order changes: every point keeps its
-// reference point index (its seed) and the min is order-free.
+// Screen bins: the splat walks a pass's survivors grouped by the 64x64 splat-buffer tile (or
+// block of tiles, for very large views) that holds their pixel mean, so that blocks running at
+// the same time write a compact part of the buffer.  Only the order changes: every point keeps
+// its reference point index (its seed) and the min is order-free.
 constexpr uint32_t kMaxBins = 16384;  // screen bins per pass (bins widen beyond 8192 x 8192 pixels)
 #ifndef GPS_SPLAT_BINNED
-#define GPS_SPLAT_BINNED 0
+#define GPS_SPLAT_BINNED 1
 #endif
-struct BinArgs {
-    const SplatRecord* records;
-    const uint32_t* surv_gid;        // Gaussian order (the scan's output)
-    const uint32_t* surv_start;      // first point (reference point index) per survivor
-    const uint32_t* counts;
-    PassCounters* counters;          // survivors and P in; binned survivors out (pad[0])
-    unsigned long long* bins;        // [nbins + 1] (survivors << 32 | points): counts, then cursors
-    uint32_t nbins;
-    int bins_x, bins_y;              // bin grid
-    int bin_shift;                   // log2 of the bin width in pixels (6 = one buffer tile)
-    int up_width, up_height;
-    uint32_t* sorted_gid;            // [n] outputs in bin order
-    uint32_t* sorted_pstart;
-    uint32_t* sorted_qstart;
-};
+GPS_HD uint32_t screen_bin(float pmx, float pmy, int up_width, int up_height, int bin_shift, int bins_x, int bins_y) {
+    const float x = fminf(fmaxf(pmx, 0.0f), (float)(up_width - 1));  // NaN -> 0
+    const float y = fminf(fmaxf(pmy, 0.0f), (float)(up_height - 1));
+    const int bx = min((int)x >> bin_shift, bins_x - 1);
+    const int by = min((int)y >> bin_shift, bins_y - 1);
+    return (uint32_t)(by * bins_x + bx);
+}
 
 struct ResolveArgs {
     const uint64_t* buffer;
@@ -177,9 +193,12 @@ void launch_encode_half(const float4* pos_op, const float4* rot, const float4* s
 void launch_translate_origins(const float4* src, uint32_t count, float dx, float dz, float4* dst, cudaStream_t stream);
 void launch_tile_nodes(const float4* src, uint32_t src_pb, uint32_t src_n, uint32_t pb, uint32_t copies,
                        const float2* offsets, uint64_t total, float4* dst, uint32_t nodes, cudaStream_t stream);
-void launch_scan(const ScanArgs& a, uint32_t scan_tiles, cudaStream_t stream, bool owners = true);
-// screen-bin the scanned survivors and find each splat tile's first survivor in that order
-void launch_bin(const BinArgs& b, const ScanArgs& a, cudaStream_t stream);
+void launch_scan(const ScanArgs& a, uint32_t scan_tiles, cudaStream_t stream);
+// The render path's scan over the tile totals the preprocess accumulated: the tile scan (and the
+// bin scan), then the downsweep that compacts the survivors, bins them and finds each splat
+// tile's first survivor.  Two launches.
+void launch_scan_fused(const ScanArgs& a, cudaStream_t stream);
+int scan_tile_shift(uint32_t n);
 uint32_t scan_tile_count(uint32_t n);
 constexpr uint32_t kScanTileGaussians = 16384;  // Gaussians per scan tile (counts are padded to it)
 void launch_splat(const SplatArgs& a, int grid, int block, cudaStream_t stream);

@@ -369,6 +369,21 @@ void render_pass(gps_renderer* r, const FrameConst& fc, int frame, bool first, c
     pa.immediate_threshold = r->s.immediate_splat_threshold;
     pa.buffer = r->buffer.get();
     pa.loaded = r->loaded.get();
+    // screen bins for this view: one 64x64 splat-buffer tile each, wider for very large views
+    const bool binned = GPS_SPLAT_BINNED != 0;
+    int bin_shift = 6;
+    while ((uint64_t)((fc.up_width + (1 << bin_shift) - 1) >> bin_shift) *
+               (uint64_t)((fc.up_height + (1 << bin_shift) - 1) >> bin_shift) > kMaxBins)
+        ++bin_shift;
+    const int bins_x = (fc.up_width + (1 << bin_shift) - 1) >> bin_shift;
+    const int bins_y = (fc.up_height + (1 << bin_shift) - 1) >> bin_shift;
+    const uint32_t nbins = (uint32_t)(bins_x * bins_y);
+    pa.tile_totals = r->tile_state.get();
+    pa.tile_shift = scan_tile_shift(r->n);
+    pa.bins = binned ? r->bins.get() : nullptr;
+    pa.bin_shift = bin_shift;
+    pa.bins_x = bins_x;
+    pa.bins_y = bins_y;
     if (r->scene->format == GPS_SCENE_FP32) {
         SceneFP32 s{r->scene->pos_op.get(), r->scene->rot.get(), r->scene->scale.get(), r->scene->sh.get(), r->n};
         launch_preprocess_fp32(pa, s, st);
@@ -402,46 +417,38 @@ void render_pass(gps_renderer* r, const FrameConst& fc, int frame, bool first, c
     sa.tile_state = r->tile_state.get();
     sa.counters = pc;
     sa.loaded = r->loaded.get();
-    const bool binned = GPS_SPLAT_BINNED != 0;
-    launch_scan(sa, r->scan_tiles, st, !binned);
-    count_launch(r, kStScan, r->scan_tiles ? 3 : 0);  // tile reduce, tile scan, downsweep
-    BinArgs b{};
-    if (binned) {
-        b.records = r->records.get();
-        b.surv_gid = r->surv_gid.get();
-        b.surv_start = r->surv_start.get();
-        b.counts = r->counts.get();
-        b.counters = pc;
-        b.bins = r->bins.get();
-        b.up_width = fc.up_width;
-        b.up_height = fc.up_height;
-        b.bin_shift = 6;  // one 64x64 splat-buffer tile per bin, coarser for very large views
-        while ((uint64_t)((fc.up_width + (1 << b.bin_shift) - 1) >> b.bin_shift) *
-                   (uint64_t)((fc.up_height + (1 << b.bin_shift) - 1) >> b.bin_shift) > kMaxBins)
-            ++b.bin_shift;
-        b.bins_x = (fc.up_width + (1 << b.bin_shift) - 1) >> b.bin_shift;
-        b.bins_y = (fc.up_height + (1 << b.bin_shift) - 1) >> b.bin_shift;
-        b.nbins = (uint32_t)(b.bins_x * b.bins_y);
-        b.sorted_gid = r->sorted_gid.get();
-        b.sorted_pstart = r->sorted_pstart.get();
-        b.sorted_qstart = r->sorted_qstart.get();
-        launch_bin(b, sa, st);
-        count_launch(r, kStScan, 4);  // bin count, bin scan, bin scatter, tile owners
-    } else {
-        count_launch(r, kStScan, r->scan_tiles ? 1 : 0);  // tile owners
-    }
+    sa.bins = binned ? r->bins.get() : nullptr;
+    sa.nbins = nbins;
+    sa.bin_shift = bin_shift;
+    sa.bins_x = bins_x;
+    sa.bins_y = bins_y;
+    sa.up_width = fc.up_width;
+    sa.up_height = fc.up_height;
+    sa.records = r->records.get();
+    sa.sorted_gid = r->sorted_gid.get();
+    sa.sorted_pstart = r->sorted_pstart.get();
+    sa.sorted_qstart = r->sorted_qstart.get();
+    launch_scan_fused(sa, st);
+    count_launch(r, kStScan, 2);  // tile (and bin) scan, downsweep with binning and tile owners
     r->timer.mark(kStSplat, st);
     SplatArgs sp{};
     sp.fc = fc;
     sp.frame_seed = frame_seed + 1;
     sp.records = r->records.get();
-    sp.surv_gid = binned ? r->sorted_gid.get() : r->surv_gid.get();
-    sp.surv_start = binned ? r->sorted_qstart.get() : r->surv_start.get();
-    sp.point_base = binned ? r->sorted_pstart.get() : nullptr;
+    sp.surv_gid = r->surv_gid.get();
+    sp.surv_start = r->surv_start.get();
+    sp.sorted_gid = binned ? r->sorted_gid.get() : nullptr;
+    sp.sorted_qstart = r->sorted_qstart.get();
+    sp.sorted_pstart = r->sorted_pstart.get();
     sp.tile_first_rank = r->tile_first_rank.get();
     sp.counters = pc;
     sp.buffer = r->buffer.get();
     sp.n = r->n;
+    sp.clear_a = r->tile_state.get();
+    sp.clear_a_words = std::max<uint32_t>(r->scan_tiles, 1);
+    sp.clear_b = binned ? r->bins.get() : nullptr;
+    sp.clear_b_words = binned ? nbins : 0u;
+    sp.mask_iter = r->mask_iter.get();
     launch_splat(sp, r->splat_grid, 256, st);
     count_launch(r, kStSplat);
 }
@@ -751,6 +758,8 @@ gps_status create_renderer(gps_scene* scene, const gps_settings* settings, const
         const uint64_t max_pts = (uint64_t)std::max(0, s.max_number_of_points);
         r->tile_first_rank.reset(dev_alloc<uint32_t>(max_pts / 256 + 2));
         r->tile_state.reset(dev_alloc<unsigned long long>(std::max<uint32_t>(r->scan_tiles, 1)));
+        // the preprocess accumulates each pass's tile totals here; the splat clears them after use
+        GPS_CUDA(cudaMemset(r->tile_state.get(), 0, sizeof(unsigned long long) * std::max<uint32_t>(r->scan_tiles, 1)));
         r->counters.reset(dev_alloc<PassCounters>(2));
         GPS_CUDA(cudaMemset(r->counters.get(), 0, sizeof(PassCounters) * 2));
         const uint32_t bwords = (r->cap_blocks + 31) / 32;

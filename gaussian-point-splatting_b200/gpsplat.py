@@ -177,6 +177,7 @@ _SIGNATURES = [
     ("gps_renderer_debug_view", c_int32, [c_void_p, POINTER(DebugView)]),
     ("gps_post_taa", c_int32, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, POINTER(c_float), c_float, c_int32, c_int32, c_int32, c_void_p]),
     ("gps_post_progressive", c_int32, [c_void_p, c_void_p, c_void_p, c_int32, c_int32, c_int32, c_void_p]),
+    ("gps_measure_atomic_min_rate", c_int32, [c_void_p, c_uint64, c_int32, POINTER(ctypes.c_double), c_void_p]),
     ("gps_workload_scan_noalloc", c_int32, [c_void_p, c_void_p, c_uint32, c_uint32, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
     ("gps_batch_create", c_int32, [c_void_p, POINTER(Settings), c_int32, c_int32, c_int32, c_int32, POINTER(c_void_p)]),
     ("gps_batch_free", None, [c_void_p]),

@@ -203,6 +203,14 @@ typedef struct gps_debug_view {
 } gps_debug_view;
 gps_status gps_renderer_debug_view(gps_renderer* r, gps_debug_view* out);
 
+/* ---- measured peaks -------------------------------------------------------------------
+ * No counterpart in the reference: the rate of 64-bit atomicMin on random addresses of a
+ * caller-owned device buffer of `entries` words (< 2^32; overwritten), best of `repeats`
+ * timed launches on `stream` (blocking).  The splat's unit of work is one such operation per
+ * live sample, so this is the roofline its achieved rate is compared with. */
+gps_status gps_measure_atomic_min_rate(uint64_t* d_buf, uint64_t entries, int32_t repeats, double* atomics_per_second,
+                                       void* stream);
+
 /* ---- allocation-free point scan ------------------------------------------------------
  * No counterpart in the reference: an extra entry point for callers that cannot allocate
  * device memory when they run the scan — inside a CUDA-graph capture or a stream-ordered
