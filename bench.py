@@ -246,19 +246,43 @@ def stage_rooflines(stages, spec, st, entries, passes, w, h, peak):
     return out
 
 
-def measured_traffic(kernel: str, spec, workload: str):
-    """DRAM bytes per launch of the dominant kernel (dram__bytes_read.sum +
-    dram__bytes_write.sum) from the committed ncu summary of the same workload, averaged over a
-    frame's launches; None when no capture of this workload is committed."""
+def profile_figure(kernel: str, workload: str, key: str):
+    """A per-launch figure of the dominant kernel from the committed ncu summary of the same
+    workload (profiles/<kernel>_traffic_<workload>.md, `key: value` lines, averaged over a
+    frame's launches): traffic_per_launch_bytes = dram__bytes_read.sum + dram__bytes_write.sum,
+    atomics_per_launch = l1tex__t_sectors_pipe_lsu_mem_global_op_red.sum.  None when absent."""
     path = os.path.join(ROOT, "profiles", f"{kernel}_traffic_{workload}.md")
     try:
         with open(path) as f:
             for ln in f:
-                if ln.startswith("traffic_per_launch_bytes:"):
+                if ln.startswith(key + ":"):
                     return float(ln.split(":")[1]), os.path.relpath(path, ROOT)
     except OSError:
         pass
     return None, None
+
+
+def measured_traffic(kernel: str, spec, workload: str):
+    return profile_figure(kernel, workload, "traffic_per_launch_bytes")
+
+
+def atomic_peaks(gpsplat, entries: int, stream):
+    """Measured rate of 64-bit atomicMin on random slots (gps_measure_atomic_min_rate): over a
+    buffer the size of the splat buffer, and over one that fits in L2."""
+    import ctypes
+
+    import torch
+
+    lib = gpsplat.load_library()
+    out = {}
+    for name, words in (("splat_buffer", entries), ("l2_resident", 8 << 20)):
+        buf = torch.empty(int(words), dtype=torch.int64, device="cuda")
+        rate = ctypes.c_double(0.0)
+        st = lib.gps_measure_atomic_min_rate(ctypes.c_void_p(buf.data_ptr()), int(words), 5, ctypes.byref(rate),
+                                             ctypes.c_void_p(stream.cuda_stream))
+        out[name] = {"atomics_per_s": rate.value if st == 0 else None, "buffer_bytes": int(words) * 8}
+        del buf
+    return out
 
 
 def host_cameras(spec, settings, poses, count, phase=0):
@@ -761,6 +785,20 @@ def main():
                 "algorithmic_bytes_per_launch": alg_bytes, "ms_per_launch": per_launch_ms,
                 "traffic_source": traffic_src}
 
+    # the splat's own bound: 64-bit atomicMin on random slots of its buffer
+    splat_atomic = None
+    if "splat" in stages:
+        peaks_atomic = atomic_peaks(gpsplat, entries, stream)
+        reds, reds_src = profile_figure("splat", args.workload, "atomics_per_launch")
+        s_ms, s_launches = stages["splat"]
+        per = s_ms / max(1, s_launches)
+        peak_rate = peaks_atomic["splat_buffer"]["atomics_per_s"]
+        splat_atomic = {"bound": "l2_atomic_min_u64", "peak": peak_rate, "peak_l2_resident": peaks_atomic["l2_resident"]["atomics_per_s"],
+                        "unit": "atomics/s", "ms_per_launch": per, "atomics_per_launch": reds, "atomics_source": reds_src,
+                        "achieved": (reds / (per / 1000.0)) if reds else None}
+        if reds and peak_rate:
+            splat_atomic["frac"] = splat_atomic["achieved"] / peak_rate
+
     l2_note = (f"inputs larger than L2: the {8 * entries / 1e6:.0f} MB splat buffer is cleared, scattered into and "
                f"resolved every frame; the preprocess reads the attributes of the Gaussians that pass the block cull "
                f"({(st.gaussians_read_one + st.gaussians_read_two) / passes / 1e6:.1f}M per pass)")
@@ -778,6 +816,7 @@ def main():
                 "d2h_bytes_per_step": h * w * 3, "ms_per_step": e2e_ms / K, "wall_s": wall_e2e},
         "gpu_launches": int(launches_per_frame * K),
         "roofline": roofline,
+        "splat_atomic_roofline": splat_atomic,
         "stages_ms_per_frame": {k: v[0] / K for k, v in stages.items()},
         "stage_rooflines": stage_rooflines(stages, spec, st, entries, passes, w, h, hbm_peak),
         "points_per_frame": [st.num_points_one, st.num_points_two],

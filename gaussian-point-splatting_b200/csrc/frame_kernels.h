@@ -158,6 +158,9 @@ constexpr uint32_t kMaxBins = 16384;  // screen bins per pass (bins widen beyond
 #ifndef GPS_SPLAT_BINNED
 #define GPS_SPLAT_BINNED 1
 #endif
+#ifndef GPS_BIN_SHIFT
+#define GPS_BIN_SHIFT 6  // log2 of the bin width in pixels: one 64x64 splat-buffer tile
+#endif
 GPS_HD uint32_t screen_bin(float pmx, float pmy, int up_width, int up_height, int bin_shift, int bins_x, int bins_y) {
     const float x = fminf(fmaxf(pmx, 0.0f), (float)(up_width - 1));  // NaN -> 0
     const float y = fminf(fmaxf(pmy, 0.0f), (float)(up_height - 1));

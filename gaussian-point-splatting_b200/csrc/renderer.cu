@@ -371,7 +371,7 @@ void render_pass(gps_renderer* r, const FrameConst& fc, int frame, bool first, c
     pa.loaded = r->loaded.get();
     // screen bins for this view: one 64x64 splat-buffer tile each, wider for very large views
     const bool binned = GPS_SPLAT_BINNED != 0;
-    int bin_shift = 6;
+    int bin_shift = GPS_BIN_SHIFT;
     while ((uint64_t)((fc.up_width + (1 << bin_shift) - 1) >> bin_shift) *
                (uint64_t)((fc.up_height + (1 << bin_shift) - 1) >> bin_shift) > kMaxBins)
         ++bin_shift;
