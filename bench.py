@@ -236,7 +236,7 @@ def stage_rooflines(stages, spec, st, entries, passes, w, h, peak):
         if b is None or ms <= 0 or launches <= 0:
             continue
         if k == "scan":
-            launches = max(1, launches // 4)  # four launches per pass scan
+            launches = max(1, launches // 2)  # two launches per pass: tile scan, downsweep
         per = ms / launches
         gbs = b / (per / 1000.0) / 1e9
         out[k] = {"achieved_gbs": gbs, "frac": gbs / peak, "ms_per_launch": per, "algorithmic_bytes": b}
