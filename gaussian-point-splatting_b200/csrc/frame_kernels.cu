@@ -249,8 +249,7 @@ __device__ __forceinline__ bool preprocess_one(const PreprocessArgs& a, const Sc
             ivec2 qmax = {pmax.x / fc.ss, pmax.y / fc.ss};
             if (hiz_occluded(a.hiz, proj_mean.z, qmin, qmax)) break;
         }
-        float kf = (float)(fc.ss * fc.ss * kPointsPerKernel);
-        if (!fc.reduce_point_count) kf = 1.0f;
+        const float kf = (float)fc.k_points;  // ss^2 x POINTS_PER_KERNEL, 1, or the K override
         uint32_t num_points;
         if (fc.use_unbiased) num_points = poisson(seed, importance);
         else num_points = (uint32_t)stochastic_round(importance, pcg2d(seed).x);
@@ -953,7 +952,8 @@ template <int K>
 #ifndef GPS_SPLAT_MIN_BLOCKS
 #define GPS_SPLAT_MIN_BLOCKS 4
 #endif
-__global__ void __launch_bounds__(kSplatTile, kSplatRounds > 1 ? GPS_SPLAT_MIN_BLOCKS : 1) splat_kernel(SplatArgs a) {
+// (K = 8 keeps two passes of eight samples in flight: more registers, fewer resident blocks)
+__global__ void __launch_bounds__(kSplatTile, kSplatRounds > 1 ? (K >= 8 ? 2 : GPS_SPLAT_MIN_BLOCKS) : 1) splat_kernel(SplatArgs a) {
     __shared__ uint32_t s_start[kSplatWindow];
     __shared__ uint32_t s_spread[kTileSize];
     if (GPS_SPLAT_MORTON_LUT && threadIdx.x < kTileSize) s_spread[threadIdx.x] = morton_spread(threadIdx.x);
@@ -1660,6 +1660,10 @@ void launch_splat(const SplatArgs& a, int grid, int block, cudaStream_t stream) 
     // a persistent grid: as many blocks as fit on the device at once
     if (a.fc.use_unbiased && a.fc.k_points == 4) {
         launch_k(splat_kernel<4>, g_num_sms * splat_blocks_per_sm<4>(), kSplatTile, 0, stream, a);
+    } else if (a.fc.use_unbiased && a.fc.k_points == 2) {
+        launch_k(splat_kernel<2>, g_num_sms * splat_blocks_per_sm<2>(), kSplatTile, 0, stream, a);
+    } else if (a.fc.use_unbiased && a.fc.k_points == 8) {
+        launch_k(splat_kernel<8>, g_num_sms * splat_blocks_per_sm<8>(), kSplatTile, 0, stream, a);
     } else if (a.fc.use_unbiased && a.fc.k_points == 1) {
         launch_k(splat_kernel<1>, g_num_sms * splat_blocks_per_sm<1>(), kSplatTile, 0, stream, a);
     } else {

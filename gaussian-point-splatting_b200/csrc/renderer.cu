@@ -308,7 +308,8 @@ FrameConst make_frame_const(const gps_renderer* r, const gps_camera* cam) {
     fc.up_height = r->up_h;
     fc.num_passes = r->s.samples_per_pixel;
     fc.ss = r->s.supersampling_factor;
-    fc.k_points = r->s.reduce_point_count ? fc.ss * fc.ss * kPointsPerKernel : 1;
+    fc.k_points = !r->s.reduce_point_count ? 1
+                  : r->s.points_per_thread > 0 ? r->s.points_per_thread : fc.ss * fc.ss * kPointsPerKernel;
     fc.near_plane = r->s.near_view_plane;
     fc.far_plane = r->s.far_view_plane;
     for (int i = 0; i < 6; ++i)
@@ -484,6 +485,7 @@ void gps_settings_default(gps_settings* s) {
     s->accumulation_mode = GPS_ACCUM_PROGRESSIVE;
     s->sort_morton_order = 0;
     s->immediate_splat_threshold = 0;
+    s->points_per_thread = 0;
 }
 
 gps_status gps_settings_parse_args(int32_t argc, const char* const* argv, gps_settings* s, char* model_path,
@@ -720,6 +722,8 @@ gps_status create_renderer(gps_scene* scene, const gps_settings* settings, const
         return fail(GPS_ERR_INVALID_ARGUMENT, "resolution, supersampling factor and samples per pixel must be positive");
     if (!(s.far_view_plane > s.near_view_plane) || !(s.fovy > 0.0f))
         return fail(GPS_ERR_INVALID_ARGUMENT, "need far > near and fovy > 0");
+    if (s.points_per_thread < 0 || s.points_per_thread > 64)
+        return fail(GPS_ERR_INVALID_ARGUMENT, "points_per_thread must be 0 (the reference's rule) or 1..64");
     const uint64_t up_w = (uint64_t)s.width * s.supersampling_factor, up_h = (uint64_t)s.height * s.supersampling_factor;
     if (up_w > 65504 || up_h > 65504) return fail(GPS_ERR_SIZE, "supersampled resolution above 65504 pixels per axis");
     const uint64_t entries = splat_buffer_entries((int)up_w, (int)up_h, s.samples_per_pixel);
@@ -1034,8 +1038,18 @@ struct gps_batch {
     std::vector<cudaEvent_t> joined;
     cudaEvent_t forked = nullptr;
     int active = 1;
+    // CUDA-graph replay: the batch's whole fork/join launch sequence, captured on a private
+    // stream; a batch with the same view layout refreshes the executable graph's parameters
+    // (cameras) with cudaGraphExecUpdate instead of instantiating a new one
+    bool use_graph = false;
+    cudaStream_t capture = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    std::vector<int64_t> exec_layout;
+    int64_t graph_instantiations = 0, graph_updates = 0;
     ~gps_batch() {
         cudaDeviceSynchronize();
+        if (exec) cudaGraphExecDestroy(exec);
+        if (capture) cudaStreamDestroy(capture);
         for (gps_renderer* w : workers) delete w;
         for (cudaStream_t st : streams) cudaStreamDestroy(st);
         for (cudaEvent_t e : joined) cudaEventDestroy(e);
@@ -1117,12 +1131,11 @@ gps_status gps_batch_set_workers(gps_batch* b, int32_t workers) {
 
 int32_t gps_batch_workers(const gps_batch* b) { return b ? b->active : 0; }
 
-gps_status gps_batch_render(gps_batch* b, const gps_view* views, int32_t count, void* stream) {
-    if (!b || (count > 0 && !views) || count < 0) return fail(GPS_ERR_INVALID_ARGUMENT, "null argument");
-    for (int i = 0; i < count; ++i)
-        if (!views[i].d_image || !views[i].d_depth) return fail(GPS_ERR_INVALID_ARGUMENT, "view without output buffers");
-    cudaStream_t st = as_stream(stream);
-    const std::vector<int> owner = assign_views(b, views, count, b->workers[0]->n);
+namespace {
+// The batch's launch sequence on `st`: fork to the workers' streams, each view as a fresh
+// renderer's first frame on its worker, join back.
+gps_status batch_enqueue(gps_batch* b, const gps_view* views, int32_t count, const std::vector<int>& owner,
+                         cudaStream_t st) {
     cudaEventRecord(b->forked, st);
     for (int w = 0; w < b->active; ++w) cudaStreamWaitEvent(b->streams[w], b->forked, 0);
     gps_status rc = GPS_OK;
@@ -1131,9 +1144,115 @@ gps_status gps_batch_render(gps_batch* b, const gps_view* views, int32_t count, 
         cudaEventRecord(b->joined[w], b->streams[w]);
         cudaStreamWaitEvent(st, b->joined[w], 0);
     }
+    return rc;
+}
+}  // namespace
+
+gps_status gps_batch_render(gps_batch* b, const gps_view* views, int32_t count, void* stream) {
+    if (!b || (count > 0 && !views) || count < 0) return fail(GPS_ERR_INVALID_ARGUMENT, "null argument");
+    for (int i = 0; i < count; ++i)
+        if (!views[i].d_image || !views[i].d_depth) return fail(GPS_ERR_INVALID_ARGUMENT, "view without output buffers");
+    cudaStream_t st = as_stream(stream);
+    const std::vector<int> owner = assign_views(b, views, count, b->workers[0]->n);
+    gps_status rc = GPS_OK;
+    if (!b->use_graph) {
+        rc = batch_enqueue(b, views, count, owner, st);
+    } else {
+        // the layout a captured graph can be refreshed for: worker count, K, and per view its
+        // size, samples and worker (the same launches in the same order)
+        std::vector<int64_t> layout = {count, b->active, b->s.points_per_thread};
+        for (int i = 0; i < count; ++i) {
+            layout.push_back(views[i].width);
+            layout.push_back(views[i].height);
+            layout.push_back(views[i].samples_per_pixel);
+            layout.push_back(owner[i]);
+        }
+        if (cudaStreamBeginCapture(b->capture, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
+            return fail(GPS_ERR_CUDA, "batch graph capture could not start");
+        rc = batch_enqueue(b, views, count, owner, b->capture);
+        cudaGraph_t g = nullptr;
+        const cudaError_t ce = cudaStreamEndCapture(b->capture, &g);
+        if (rc == GPS_OK && (ce != cudaSuccess || !g)) rc = fail(GPS_ERR_CUDA, std::string("batch graph capture failed: ") + cudaGetErrorString(ce));
+        if (rc == GPS_OK && b->exec && layout == b->exec_layout) {
+            cudaGraphExecUpdateResultInfo info{};
+            if (cudaGraphExecUpdate(b->exec, g, &info) == cudaSuccess) {
+                ++b->graph_updates;
+            } else {
+                cudaGetLastError();
+                cudaGraphExecDestroy(b->exec);
+                b->exec = nullptr;
+            }
+        } else if (rc == GPS_OK && b->exec) {
+            cudaGraphExecDestroy(b->exec);
+            b->exec = nullptr;
+        }
+        if (rc == GPS_OK && !b->exec) {
+            if (cudaGraphInstantiate(&b->exec, g, 0) != cudaSuccess) {
+                b->exec = nullptr;
+                rc = fail(GPS_ERR_CUDA, "batch graph instantiation failed");
+            } else {
+                b->exec_layout = layout;
+                ++b->graph_instantiations;
+            }
+        }
+        if (g) cudaGraphDestroy(g);
+        if (rc == GPS_OK && cudaGraphLaunch(b->exec, st) != cudaSuccess) rc = fail(GPS_ERR_CUDA, "batch graph launch failed");
+    }
     if (rc != GPS_OK) return rc;
     cudaError_t e = cudaGetLastError();
     return e == cudaSuccess ? GPS_OK : fail(GPS_ERR_CUDA, std::string("batch launch failed: ") + cudaGetErrorString(e));
+}
+
+gps_status gps_batch_use_graph(gps_batch* b, int32_t enable) {
+    if (!b) return fail(GPS_ERR_INVALID_ARGUMENT, "null argument");
+    if (enable && !b->capture && cudaStreamCreateWithFlags(&b->capture, cudaStreamNonBlocking) != cudaSuccess)
+        return fail(GPS_ERR_CUDA, "stream creation failed");
+    b->use_graph = enable != 0;
+    return GPS_OK;
+}
+
+gps_status gps_batch_graph_stats(const gps_batch* b, int64_t* instantiations, int64_t* updates) {
+    if (!b) return fail(GPS_ERR_INVALID_ARGUMENT, "null argument");
+    if (instantiations) *instantiations = b->graph_instantiations;
+    if (updates) *updates = b->graph_updates;
+    return GPS_OK;
+}
+
+gps_status gps_batch_set_points_per_thread(gps_batch* b, int32_t k) {
+    if (!b || k < 0 || k > 64) return fail(GPS_ERR_INVALID_ARGUMENT, "points_per_thread must be 0..64");
+    b->s.points_per_thread = k;
+    for (gps_renderer* w : b->workers) w->s.points_per_thread = k;
+    return GPS_OK;
+}
+
+gps_status gps_batch_autotune_k(gps_batch* b, const gps_view* views, int32_t count, int32_t rounds, void* stream,
+                                int32_t* chosen_workers, int32_t* chosen_k, float* ms) {
+    if (!b || rounds < 1) return fail(GPS_ERR_INVALID_ARGUMENT, "bad argument");
+    const int32_t ks[] = {1, 2, 4, 8};
+    int best_w = 1, best_k = b->s.points_per_thread;
+    float best_ms = 0.0f;
+    bool have = false;
+    gps_status rc = GPS_OK;
+    for (int32_t k : ks) {
+        rc = gps_batch_set_points_per_thread(b, k);
+        if (rc != GPS_OK) break;
+        int32_t w = 1;
+        float t = 0.0f;
+        rc = gps_batch_autotune(b, views, count, rounds, stream, &w, &t);
+        if (rc != GPS_OK) break;
+        if (!have || t < best_ms) {
+            have = true;
+            best_w = w;
+            best_k = k;
+            best_ms = t;
+        }
+    }
+    gps_batch_set_points_per_thread(b, best_k);
+    b->active = best_w;
+    if (chosen_workers) *chosen_workers = best_w;
+    if (chosen_k) *chosen_k = best_k;
+    if (ms) *ms = best_ms;
+    return rc;
 }
 
 gps_status gps_batch_autotune(gps_batch* b, const gps_view* views, int32_t count, int32_t rounds, void* stream,

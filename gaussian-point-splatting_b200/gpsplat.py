@@ -69,6 +69,7 @@ class Settings(ctypes.Structure):
         ("accumulation_mode", c_int32),
         ("sort_morton_order", c_int32),
         ("immediate_splat_threshold", c_int32),
+        ("points_per_thread", c_int32),
     ]
 
 
@@ -185,6 +186,10 @@ _SIGNATURES = [
     ("gps_batch_set_workers", c_int32, [c_void_p, c_int32]),
     ("gps_batch_workers", c_int32, [c_void_p]),
     ("gps_batch_autotune", c_int32, [c_void_p, POINTER(View), c_int32, c_int32, c_void_p, POINTER(c_int32), POINTER(c_float)]),
+    ("gps_batch_autotune_k", c_int32, [c_void_p, POINTER(View), c_int32, c_int32, c_void_p, POINTER(c_int32), POINTER(c_int32), POINTER(c_float)]),
+    ("gps_batch_set_points_per_thread", c_int32, [c_void_p, c_int32]),
+    ("gps_batch_use_graph", c_int32, [c_void_p, c_int32]),
+    ("gps_batch_graph_stats", c_int32, [c_void_p, POINTER(ctypes.c_int64), POINTER(ctypes.c_int64)]),
     ("gps_server_create", c_int32, [POINTER(c_void_p), c_int32, POINTER(Settings), c_int32, c_int32, c_int32, c_int32, POINTER(c_void_p)]),
     ("gps_server_set_admission", c_int32, [c_void_p, c_uint64]),
     ("gps_server_submit", c_int32, [c_void_p, POINTER(Request)]),
@@ -481,6 +486,24 @@ class Batch:
         _check(load_library().gps_batch_autotune(self._h, views, len(views), rounds, c_void_p(stream), byref(chosen),
                                                  byref(ms)))
         return chosen.value, ms.value
+
+    def autotune_k(self, views, rounds: int = 2, stream: int = 0):
+        """K in {1, 2, 4, 8} x worker count; returns (workers, K, ms per batch)."""
+        w, k, ms = c_int32(), c_int32(), c_float()
+        _check(load_library().gps_batch_autotune_k(self._h, views, len(views), rounds, c_void_p(stream), byref(w), byref(k),
+                                                   byref(ms)))
+        return w.value, k.value, ms.value
+
+    def set_points_per_thread(self, k: int):
+        _check(load_library().gps_batch_set_points_per_thread(self._h, k))
+
+    def use_graph(self, enable: bool = True):
+        _check(load_library().gps_batch_use_graph(self._h, int(enable)))
+
+    def graph_stats(self):
+        inst, upd = ctypes.c_int64(), ctypes.c_int64()
+        _check(load_library().gps_batch_graph_stats(self._h, byref(inst), byref(upd)))
+        return inst.value, upd.value
 
     def close(self):
         if self._h:

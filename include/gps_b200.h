@@ -79,6 +79,12 @@ typedef struct gps_settings {
      * reference compiles the option out by default, hence 0 = off here; its menu default,
      * when compiled in, is 8. */
     int32_t immediate_splat_threshold;          /* 0 */
+    /* points_per_thread (K): not in the reference, which fixes K = ss^2 x POINTS_PER_KERNEL
+     * (1 with reduce_point_count off).  > 0 overrides it: a Gaussian's Poisson count is divided
+     * by K and each point draws K samples per spp pass, so the estimator is unchanged and the
+     * work moves between points and samples (the batch autotuner's knob).  0 = the reference's
+     * rule; renders with the same K are bit-identical to each other. */
+    int32_t points_per_thread;                  /* 0 */
 } gps_settings;
 
 /* One frame's camera: what RenderSettings carries per frame (render_settings.cuh:94-105). */
@@ -266,6 +272,20 @@ gps_status gps_batch_render(gps_batch* b, const gps_view* views, int32_t count, 
 /* Number of workers used by gps_batch_render (1 .. the number created). */
 gps_status gps_batch_set_workers(gps_batch* b, int32_t workers);
 int32_t gps_batch_workers(const gps_batch* b);
+/* Points per thread K of every view (gps_settings.points_per_thread; 0 = the reference's rule).
+ * Each view stays bit-identical to a plain render with the same K. */
+gps_status gps_batch_set_points_per_thread(gps_batch* b, int32_t k);
+/* enable != 0: gps_batch_render replays the batch from a CUDA graph: the fork/join launch
+ * sequence is captured on a private stream, and a batch whose layout (view sizes, samples,
+ * worker assignment, K) matches the previous one updates the executable graph's parameters
+ * (the cameras) with cudaGraphExecUpdate instead of instantiating it again; the graph is
+ * launched on the caller's stream.  Results are identical to the direct launches. */
+gps_status gps_batch_use_graph(gps_batch* b, int32_t enable);
+gps_status gps_batch_graph_stats(const gps_batch* b, int64_t* instantiations, int64_t* updates);
+/* The autotuner over K in {1, 2, 4, 8} and, for each, the worker count (gps_batch_autotune);
+ * leaves the batch at the fastest pair. */
+gps_status gps_batch_autotune_k(gps_batch* b, const gps_view* views, int32_t count, int32_t rounds, void* stream,
+                                int32_t* chosen_workers, int32_t* chosen_k, float* ms);
 /* Autotuner: times `rounds` renders of the batch for each worker count 1, 2, 4, ... up to the
  * number created (CUDA events on `stream`), keeps the fastest and returns it in *chosen and its
  * time per batch in *ms (either may be NULL).  Synchronises `stream`. */

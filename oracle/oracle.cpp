@@ -602,7 +602,7 @@ uint32_t preprocess_one(Ctx& c, const FrameC& f, uint32_t idx, int frame_seed, b
     const int ss = s.supersampling_factor;
     if (s.enable_occlusion_culling && hiz_occluded(c.hiz, ndc_z, r.mnx / ss, r.mny / ss, r.mxx / ss, r.mxy / ss))
         return 0;
-    real k = (real)(ss * ss);
+    real k = (real)(s.points_per_thread > 0 ? s.points_per_thread : ss * ss);
     if (!s.reduce_point_count) k = 1.0f;
     uint32_t n = s.use_unbiased_2d_splatting ? poisson(seed, importance) : (uint32_t)stochastic_round(importance, pcg2d(seed).x);
     if (k > 1) n = (uint32_t)stochastic_round((real)n / k, pcg2d(seed).x);
@@ -677,7 +677,7 @@ inline void atomic_add_color(uint64_t* p, uint64_t v) {
 // One point's samples from `seed` onwards (splatGaussianPoint's inner loop, :98-139).
 void splat_samples(Ctx& c, Seed& seed, const Record& r) {
     const gps_settings& s = c.s;
-    int k = s.reduce_point_count ? s.supersampling_factor * s.supersampling_factor : 1;
+    int k = !s.reduce_point_count ? 1 : s.points_per_thread > 0 ? s.points_per_thread : s.supersampling_factor * s.supersampling_factor;
     const int np = s.samples_per_pixel;
     const uint64_t vdb = r.key & (0xFFFFFFFull << 36);
     for (int q = 0; q < np * k; ++q) {

@@ -131,7 +131,7 @@ def settings_host(**overrides):
              fovy=45.0, near_view_plane=0.2, far_view_plane=10000.0, enable_hierarchical_culling=1,
              fully_disable_hierarchical_culling=0, enable_occlusion_culling=1, occlusion_culling_min_reduce_count=0,
              cull_small_gaussians=0, use_unbiased_2d_splatting=1, reduce_point_count=1, accumulation_mode=0,
-             sort_morton_order=0, immediate_splat_threshold=0)
+             sort_morton_order=0, immediate_splat_threshold=0, points_per_thread=0)
     d.update(overrides)
     for k, v in d.items():
         if k == "background":

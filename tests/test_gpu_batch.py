@@ -135,3 +135,76 @@ def test_frame_loop_async_readback_matches_blocking_read():
     assert np.array_equal(host[(n - 2) % 2].numpy(), want[-2])
     for obj in (la, lb, ra, rb, scene):
         obj.close()
+
+
+@pytest.mark.parametrize("k", [1, 2, 8])
+def test_batch_with_points_per_thread_matches_plain_at_same_k(k):
+    """K (points_per_thread, not in the reference) moves work between points and samples; a
+    batch view rendered with K is bit-identical to a plain render with the same K, and a
+    different K gives a different sample stream of the same estimator."""
+    import torch
+
+    ply = gpsutil.cached_ply("town60k", lambda: synth.town(60000, seed=5))
+    scene = gpsplat.Scene.from_ply(ply)
+    base = dict(supersampling_factor=2, max_number_of_points=4_000_000, points_per_thread=k)
+    views = _views(6, seed=40 + k)
+    plain = [_plain(scene, base, v) for v in views]
+    s = gpsplat.default_settings(**base, width=640, height=360, samples_per_pixel=8)
+    batch = gpsplat.Batch(scene, s, 640, 360, 8, workers=2)
+    batch.set_points_per_thread(k)
+    bufs = [(torch.empty((v[2], v[1], 3), device="cuda"), torch.empty((v[2], v[1]), device="cuda")) for v in views]
+    arr = gpsplat.Batch.views([(plain[i][0], v[1], v[2], v[3], bufs[i][0].data_ptr(), bufs[i][1].data_ptr())
+                               for i, v in enumerate(views)])
+    batch.render(arr)
+    torch.cuda.synchronize()
+    for i in range(len(views)):
+        assert np.array_equal(bufs[i][0].cpu().numpy().view(np.uint32), plain[i][1].view(np.uint32)), f"K={k} view {i}"
+        assert np.array_equal(bufs[i][1].cpu().numpy().view(np.uint32), plain[i][2].view(np.uint32)), f"K={k} view {i}"
+    # the reference's K (= ss^2 = 4) samples differently but estimates the same image
+    ref = _plain(scene, dict(supersampling_factor=2, max_number_of_points=4_000_000), views[0])
+    assert not np.array_equal(ref[1], plain[0][1])
+    assert abs(float(ref[1].mean()) - float(plain[0][1].mean())) < 0.02
+    batch.close()
+    scene.close()
+
+
+def test_batch_graph_replay_matches_direct_launches():
+    """The CUDA-graph replay of a batch: the first batch instantiates the graph, a second batch
+    with the same layout and new cameras updates it in place; both match plain renders bit for
+    bit, and a batch of another layout instantiates a new graph."""
+    import torch
+
+    ply = gpsutil.cached_ply("town60k", lambda: synth.town(60000, seed=5))
+    scene = gpsplat.Scene.from_ply(ply)
+    base = dict(supersampling_factor=2, max_number_of_points=4_000_000)
+    s = gpsplat.default_settings(**base, width=640, height=360, samples_per_pixel=8)
+    batch = gpsplat.Batch(scene, s, 640, 360, 8, workers=3)
+    batch.use_graph(True)
+    layout = _views(8, seed=70)
+    for call, seed in enumerate((71, 72)):
+        poses = synth.random_poses(len(layout), seed=seed)
+        views = [(poses[i], w, h, spp, frame) for i, (_, w, h, spp, frame) in enumerate(layout)]
+        plain = [_plain(scene, base, v) for v in views]
+        bufs = [(torch.empty((v[2], v[1], 3), device="cuda"), torch.empty((v[2], v[1]), device="cuda")) for v in views]
+        arr = gpsplat.Batch.views([(plain[i][0], v[1], v[2], v[3], bufs[i][0].data_ptr(), bufs[i][1].data_ptr())
+                                   for i, v in enumerate(views)])
+        batch.render(arr)
+        torch.cuda.synchronize()
+        for i in range(len(views)):
+            assert np.array_equal(bufs[i][0].cpu().numpy().view(np.uint32), plain[i][1].view(np.uint32)), f"call {call} view {i}"
+            assert np.array_equal(bufs[i][1].cpu().numpy().view(np.uint32), plain[i][2].view(np.uint32)), f"call {call} view {i}"
+    assert batch.graph_stats() == (1, 1), batch.graph_stats()
+    other = _views(5, seed=73)
+    plain = [_plain(scene, base, v) for v in other]
+    bufs = [(torch.empty((v[2], v[1], 3), device="cuda"), torch.empty((v[2], v[1]), device="cuda")) for v in other]
+    arr = gpsplat.Batch.views([(plain[i][0], v[1], v[2], v[3], bufs[i][0].data_ptr(), bufs[i][1].data_ptr())
+                               for i, v in enumerate(other)])
+    batch.render(arr)
+    torch.cuda.synchronize()
+    assert batch.graph_stats()[0] == 2
+    for i in range(len(other)):
+        assert np.array_equal(bufs[i][0].cpu().numpy().view(np.uint32), plain[i][1].view(np.uint32))
+    w, k, ms = batch.autotune_k(arr, rounds=1)
+    assert k in (1, 2, 4, 8) and 1 <= w <= 3 and ms > 0
+    batch.close()
+    scene.close()
