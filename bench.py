@@ -205,7 +205,7 @@ def barrier(world: int):
 # bytes the preprocess reads per Gaussian it loads (opacity + geometry) and per survivor (SH),
 # by scene format: FP32 SoA (16 B position+opacity, 16 B rotation, 16 B scale; 192 B SH),
 # the reference's compressed format (16 B quantised geometry + 1 B opacity; 64 B compact SH),
-# and the half format (16 B + 16 B records; 48 B FP8 AC coefficients)
+# and the half format (16 B + 16 B records; 48 B int8 AC coefficients)
 PREPROCESS_BYTES = {"fp32": (48.0, 192.0), "compressed": (17.0, 64.0), "half": (32.0, 48.0)}
 
 
@@ -398,10 +398,51 @@ def reference_cuda(gpsplat, ply, spec, settings, cams, warmup, mine_ms):
             continue
         ref = json.loads([ln for ln in res.stdout.splitlines() if ln.startswith("{")][-1])
         entry = {"reference_ms_per_frame": ref["ms_per_frame"], "frames": ref["frames"], "wall_s": time.time() - t}
+        ready = [ln for ln in res.stderr.splitlines() if ln.startswith("reference scene ready in")]
+        if ready:  # the reference's PLY load + scene upload + BVH build (its GaussianPointSplatting constructor)
+            entry["reference_scene_load_s"] = float(ready[-1].split()[4])
         if mine_ms.get(variant):
             entry["ms_per_frame"] = mine_ms[variant]
             entry["speedup"] = ref["ms_per_frame"] / mine_ms[variant]
         out[variant] = entry
+    return out
+
+
+def ingest(gpsplat, ply, g_host, load_ply_s):
+    """The load path around the frame path: PLY parse, the scene build through the PLY loader,
+    and the --sort-morton-order reorder (gaussian_loader.cu:363-424) on the host (the
+    reference's host keys + sort) and on the device (keys, stable radix sort and gather in HBM),
+    on the workload's own Gaussians in a shuffled order."""
+    import torch
+
+    n = g_host.shape[0]
+    out = {"gaussians": n, "load_ply_s": load_ply_s}
+    t = time.perf_counter()
+    gpsplat.ply_read(ply)
+    out["ply_parse_s"] = time.perf_counter() - t
+    perm = np.random.default_rng(0x5EED).permutation(n)
+    shuffled = np.ascontiguousarray(g_host[perm])
+    t = time.perf_counter()
+    host_order = gpsplat.morton_order(shuffled, on_device=False)
+    out["morton_order_host_s"] = time.perf_counter() - t
+    gpsplat.morton_order(shuffled[: 1 << 16], on_device=True)  # first-use costs outside the timing
+    t = time.perf_counter()
+    dev_order = gpsplat.morton_order(shuffled, on_device=True)
+    out["morton_order_device_s"] = time.perf_counter() - t
+    out["orders_equal"] = bool(np.array_equal(host_order, dev_order))
+    del host_order, dev_order
+    for mode, key in ((1, "scene_build_host_reorder_s"), (2, "scene_build_device_reorder_s")):
+        torch.cuda.synchronize()
+        t = time.perf_counter()
+        sc = gpsplat.Scene.from_host_sorted(shuffled, gpsplat.GPS_SCENE_FP32, mode)
+        torch.cuda.synchronize()
+        out[key] = time.perf_counter() - t
+        sc.close()
+    t = time.perf_counter()
+    sc = gpsplat.Scene.from_host(shuffled, gpsplat.GPS_SCENE_FP32, presorted=False)
+    torch.cuda.synchronize()
+    out["scene_build_no_reorder_s"] = time.perf_counter() - t
+    sc.close()
     return out
 
 
@@ -638,7 +679,7 @@ def run_serve_workload(args, world, rank, local):
     line = {
         "metric": "served views/sec", "value": top["views_per_s"] * world, "unit": "views/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 / top["views_per_s"] * 20,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32 (16M town), f16/fp8 storage (256M town)",
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32 (16M town), f16/int8 storage (256M town)",
         "data": "synthetic (seeded towns, poses and Poisson arrivals, see synth.py)",
         "config": {"workload": "serve", "requests_per_rate": len(reqs), "scenes": {"town16m_fp32": 0.7, "town256m_half": 0.3},
                    "resolutions": SERVE_RES, "spp": SERVE_SPP, "supersampling": 2, "rates_req_s": SERVE_RATES,
@@ -668,6 +709,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-reference-cuda", action="store_true", help="skip timing the reference's CUDA build")
     ap.add_argument("--quick-cpu", action="store_true", help="CPU baseline on all cores only (no 1-thread frame)")
+    ap.add_argument("--no-ingest", action="store_true", help="skip timing the PLY parse and the Morton reorder")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     world, rank, local = dist_init()
@@ -706,7 +748,8 @@ def main():
     else:
         # through the reference-facing loader (gps_scene_load_ply), as a drop-in user loads it
         scene = gpsplat.Scene.from_ply(ply, gpsplat.GPS_SCENE_FP32)
-    log(f"rank {rank}: scene uploaded in {time.time() - t:.1f}s")
+    load_ply_s = time.time() - t
+    log(f"rank {rank}: scene uploaded in {load_ply_s:.1f}s")
     s = settings_for(gpsplat, spec)
     r = gpsplat.Renderer(scene, s)
     loop = gpsplat.FrameLoop(r)
@@ -845,9 +888,10 @@ def main():
         "points_per_frame": [st.num_points_one, st.num_points_two],
         "survivors_per_frame": [st.survivors_one, st.survivors_two],
         "gaussians_read_per_frame": [st.gaussians_read_one, st.gaussians_read_two],
+        "screen_order_per_pass": [st.screen_order_one, st.screen_order_two],
     }
     if spec.get("fmt") == "half":
-        line["dtype"] = "f16/fp8 storage, f32 arithmetic"
+        line["dtype"] = "f16/int8 storage, f32 arithmetic"
         line["config"]["format"] = "half (GPS_SCENE_HALF), town tiled %dx%d" % (spec["tiles"], spec["tiles"])
     loop.close()
     r.close()
@@ -859,6 +903,8 @@ def main():
         mine["compressed"] = time_frames(gpsplat, comp, s, cams, args.warmup, stream)
         comp.close()
         line["reference_cuda"] = reference_cuda(gpsplat, ply, spec, s, cams, args.warmup, mine)
+    if rank == 0 and world == 1 and spec.get("fmt") != "half" and not args.no_ingest:
+        line["ingest"] = ingest(gpsplat, ply, g_host, load_ply_s)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         if spec.get("fmt") == "half":
             line["cpu_baseline"] = {"value": None, "unit": "Gaussians/s", "cores": os.cpu_count() or 1, "kind": "port",

@@ -472,10 +472,12 @@ constexpr int kTileScanPer = 4;
 // One block: exclusive prefix of `count` packed (survivors << 32 | points) words in place,
 // through shared memory in coalesced rounds; returns the totals.
 __device__ __forceinline__ void scan_words_inplace(unsigned long long* words_g, uint32_t count, uint32_t& total_s,
-                                                   uint32_t& total_p) {
+                                                   uint32_t& total_p, uint32_t* max_s = nullptr) {
     __shared__ unsigned long long words[kTileScanThreads * kTileScanPer];
+    __shared__ uint32_t s_max;
     constexpr uint32_t kRound = kTileScanThreads * kTileScanPer;
-    uint32_t carry_s = 0, carry_p = 0;
+    uint32_t carry_s = 0, carry_p = 0, my_max = 0;
+    if (threadIdx.x == 0) s_max = 0;
     for (uint32_t r0 = 0; r0 < count; r0 += kRound) {
         for (uint32_t i = threadIdx.x; i < kRound; i += kTileScanThreads)
             words[i] = r0 + i < count ? words_g[r0 + i] : 0ull;
@@ -486,6 +488,7 @@ __device__ __forceinline__ void scan_words_inplace(unsigned long long* words_g, 
             const unsigned long long v = words[threadIdx.x * kTileScanPer + k];
             s += (uint32_t)(v >> 32);
             p += (uint32_t)v;
+            my_max = max(my_max, (uint32_t)(v >> 32));
         }
         uint32_t ex_s, ex_p, tot_s, tot_p;
         block_scan_pair<kTileScanThreads>(s, p, ex_s, ex_p, tot_s, tot_p);
@@ -506,6 +509,12 @@ __device__ __forceinline__ void scan_words_inplace(unsigned long long* words_g, 
     }
     total_s = carry_s;
     total_p = carry_p;
+    if (max_s) {  // the largest survivor count of one word
+        my_max = __reduce_max_sync(0xffffffffu, my_max);
+        if ((threadIdx.x & 31u) == 0u) atomicMax(&s_max, my_max);
+        __syncthreads();
+        *max_s = s_max;
+    }
 }
 
 // Pass 2: block 0 turns the tile totals into exclusive tile prefixes (in place) and writes the
@@ -514,7 +523,11 @@ __device__ __forceinline__ void scan_words_inplace(unsigned long long* words_g, 
 __global__ void __launch_bounds__(kTileScanThreads) scan_tiles_kernel(ScanArgs a, uint32_t num_tiles) {
     uint32_t carry_s, carry_p;
     if (blockIdx.x == 1) {
-        scan_words_inplace(a.bins, a.nbins, carry_s, carry_p);
+        uint32_t most = 0;
+        scan_words_inplace(a.bins, a.nbins, carry_s, carry_p, &most);
+        // a bin crowded past bin_crowded survivors would serialise the downsweep on its cursor:
+        // the pass is then walked in Gaussian order
+        if (threadIdx.x == 0) a.counters->crowded = most > a.bin_crowded ? 1u : 0u;
         return;
     }
     scan_words_inplace(a.tile_state, num_tiles, carry_s, carry_p);
@@ -526,7 +539,8 @@ __global__ void __launch_bounds__(kTileScanThreads) scan_tiles_kernel(ScanArgs a
         a.counters->scan_timeouts = 0u;
         a.counters->loaded = a.loaded ? *a.loaded : 0u;
         if (a.loaded) *a.loaded = 0u;  // the next pass's preprocess tallies from zero
-        a.counters->pad[0] = a.counters->pad[1] = 0u;
+        a.counters->pad = 0u;
+        if (!a.bins) a.counters->crowded = 0u;
     }
 }
 
@@ -599,7 +613,7 @@ __global__ void __launch_bounds__(kScanThreads) scan_write_fused_kernel(ScanArgs
     block_scan_pair<kScanThreads>(surv, pts, ex_s, ex_p, tot_s, tot_p);
     if (surv == 0u) return;
     const uint32_t P = a.counters->points;
-    const bool binned = a.bins && a.counters->truncated == 0u;
+    const bool binned = a.bins && a.counters->truncated == 0u && a.counters->crowded == 0u;
     const unsigned long long pre = a.tile_state[tile];
     uint32_t r = (uint32_t)(pre >> 32) + ex_s;
     uint32_t pt = (uint32_t)pre + ex_p;
@@ -959,8 +973,9 @@ __global__ void __launch_bounds__(kSplatTile, kSplatRounds > 1 ? (K >= 8 ? 2 : G
     if (GPS_SPLAT_MORTON_LUT && threadIdx.x < kTileSize) s_spread[threadIdx.x] = morton_spread(threadIdx.x);
     const uint32_t points = a.counters->points;
     const uint32_t survivors = a.counters->survivors;
-    // the pass's work order: screen bins unless the scan had to truncate the pass
-    const bool binned = a.sorted_gid && a.counters->truncated == 0u;
+    // the pass's work order: screen bins unless the scan had to truncate the pass or a bin was
+    // too crowded to sort into
+    const bool binned = a.sorted_gid && a.counters->truncated == 0u && a.counters->crowded == 0u;
     const uint32_t* __restrict__ gids = binned ? a.sorted_gid : a.surv_gid;
     const uint32_t* __restrict__ first_q = binned ? a.sorted_qstart : a.surv_start;
     const uint32_t* __restrict__ point_base = binned ? a.sorted_pstart : nullptr;
@@ -1292,7 +1307,8 @@ __device__ __forceinline__ uint32_t pack_h2(float lo, float hi) {
     return (uint32_t)__half_as_ushort(__float2half_rn(lo)) | ((uint32_t)__half_as_ushort(__float2half_rn(hi)) << 16);
 }
 
-// origin of every kHalfOriginBlock Gaussians: the centre of their means' bounding box
+// origin of every kHalfOriginBlock Gaussians: the centre of their means' bounding box, and in w
+// the step of the 16-bit fixed-point offsets from it (the largest half-extent / 32767)
 __global__ void half_origins_kernel(const float4* __restrict__ pos_op, uint32_t n, float4* __restrict__ origin) {
     const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
     const uint32_t begin = b * kHalfOriginBlock;
@@ -1304,7 +1320,16 @@ __global__ void half_origins_kernel(const float4* __restrict__ pos_op, uint32_t 
         lo = make_float3(fminf(lo.x, p.x), fminf(lo.y, p.y), fminf(lo.z, p.z));
         hi = make_float3(fmaxf(hi.x, p.x), fmaxf(hi.y, p.y), fmaxf(hi.z, p.z));
     }
-    origin[b] = make_float4(0.5f * (lo.x + hi.x), 0.5f * (lo.y + hi.y), 0.5f * (lo.z + hi.z), 0.0f);
+    const float3 o = make_float3(0.5f * (lo.x + hi.x), 0.5f * (lo.y + hi.y), 0.5f * (lo.z + hi.z));
+    const float h = fmaxf(fmaxf(fmaxf(hi.x - o.x, o.x - lo.x), fmaxf(hi.y - o.y, o.y - lo.y)),
+                          fmaxf(hi.z - o.z, o.z - lo.z));
+    const float k = __fdiv_rn(h, 32767.0f);
+    origin[b] = make_float4(o.x, o.y, o.z, k >= 1.0e-30f ? k : 0.0f);
+}
+
+__device__ __forceinline__ uint32_t fixed16(float v, float o, float k) {
+    const int q = k > 0.0f ? max(-32767, min(32767, __float2int_rn(__fdiv_rn(v - o, k)))) : 0;
+    return (uint32_t)q & 0xFFFFu;
 }
 
 __global__ void encode_half_kernel(const float4* __restrict__ pos_op, const float4* __restrict__ rot,
@@ -1314,7 +1339,9 @@ __global__ void encode_half_kernel(const float4* __restrict__ pos_op, const floa
     const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
     if (g >= n) return;
     const float4 p = pos_op[g], q = rot[g], c = scale[g], o = origin[g / kHalfOriginBlock];
-    rec[g] = make_uint4(pack_h2(p.x - o.x, p.y - o.y), pack_h2(p.z - o.z, p.w), pack_h2(q.x, q.y), pack_h2(q.z, q.w));
+    const uint32_t op16 = (uint32_t)__half_as_ushort(__float2half_rn(p.w));
+    rec[g] = make_uint4(fixed16(p.x, o.x, o.w) | (fixed16(p.y, o.y, o.w) << 16), fixed16(p.z, o.z, o.w) | (op16 << 16),
+                        pack_h2(q.x, q.y), pack_h2(q.z, q.w));
     float v[48];
 #pragma unroll
     for (int i = 0; i < 12; ++i) {
@@ -1324,19 +1351,33 @@ __global__ void encode_half_kernel(const float4* __restrict__ pos_op, const floa
         v[4 * i + 2] = t.z;
         v[4 * i + 3] = t.w;
     }
-    float m = 0.0f;
+    // AC terms: 8-bit integers on a per-band scale (band 1: AC 0-8, band 2: 9-23, band 3: 24-44),
+    // scale = the band's max |c| / 127 rounded up to bf16, so that every |c| / scale <= 127
+    float mb[3] = {0.0f, 0.0f, 0.0f};
 #pragma unroll
-    for (int j = 3; j < 48; ++j) m = fmaxf(m, fabsf(v[j]));
-    const float k = m > 0.0f ? m / 448.0f : 1.0f;   // 448 = largest finite e4m3 value
-    scl[g] = make_uint4(pack_h2(c.x, c.y), pack_h2(c.z, v[0]), pack_h2(v[1], v[2]), __float_as_uint(k));
+    for (int e = 0; e < 45; ++e) {
+        const int b = e < 9 ? 0 : (e < 24 ? 1 : 2);
+        mb[b] = fmaxf(mb[b], fabsf(v[3 + e]));
+    }
+    uint32_t sb[3];
+    float sc[3];
+#pragma unroll
+    for (int b = 0; b < 3; ++b) {
+        const uint32_t bits = __float_as_uint(mb[b] / 127.0f);
+        sb[b] = (bits >> 16) + ((bits & 0xFFFFu) ? 1u : 0u);
+        sc[b] = __uint_as_float(sb[b] << 16);
+    }
+    scl[g] = make_uint4(pack_h2(c.x, c.y), pack_h2(c.z, v[0]), pack_h2(v[1], v[2]), sb[0] | (sb[1] << 16));
     uint32_t w[12];
 #pragma unroll
     for (int i = 0; i < 12; ++i) w[i] = 0u;
 #pragma unroll
-    for (int j = 0; j < 45; ++j) {
-        const uint32_t b = (uint32_t)__nv_cvt_float_to_fp8(v[3 + j] / k, __NV_SATFINITE, __NV_E4M3);
-        w[j >> 2] |= b << (8 * (j & 3));
+    for (int e = 0; e < 45; ++e) {
+        const float k = sc[e < 9 ? 0 : (e < 24 ? 1 : 2)];
+        const int q = k > 0.0f ? max(-127, min(127, __float2int_rn(__fdiv_rn(v[3 + e], k)))) : 0;
+        w[e >> 2] |= ((uint32_t)q & 0xFFu) << (8 * (e & 3));
     }
+    w[11] |= sb[2] << 8;  // bytes 45-46: band 3's scale
 #pragma unroll
     for (int i = 0; i < 3; ++i) acq[(size_t)g * 3 + i] = make_uint4(w[4 * i], w[4 * i + 1], w[4 * i + 2], w[4 * i + 3]);
 }
@@ -1894,3 +1935,128 @@ extern "C" gps_status gps_workload_scan_noalloc(const uint32_t* d_counts, const 
     }
     return GPS_OK;
 }
+
+// ---------------------------------------------------------------------------------
+// Scene order on the device: 3D Morton order of the Gaussian means, the same order as the host
+// reorder (host_scene.cpp morton_sort: keys from the scene's bounding box, 21 bits per axis,
+// a stable sort), computed with round-to-nearest arithmetic so that every key is the host's.
+// ---------------------------------------------------------------------------------
+#include <cub/device/device_radix_sort.cuh>
+
+namespace gps {
+namespace {
+
+__device__ __forceinline__ uint32_t ordered_bits(float f) {  // monotone float -> uint32 map
+    const uint32_t b = __float_as_uint(f);
+    return (b & 0x80000000u) ? ~b : (b | 0x80000000u);
+}
+__device__ __forceinline__ float from_ordered_bits(uint32_t b) {
+    return __uint_as_float((b & 0x80000000u) ? (b & 0x7FFFFFFFu) : ~b);
+}
+
+__global__ void __launch_bounds__(256) mean_bounds_kernel(const float4* __restrict__ pos, uint32_t n,
+                                                          uint32_t* __restrict__ bounds6) {
+    uint32_t lo[3] = {0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu}, hi[3] = {0u, 0u, 0u};
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const float4 p = __ldg(pos + i);
+        const float f[3] = {p.x, p.y, p.z};
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            if (f[c] != f[c]) continue;  // NaN never wins the host's comparisons
+            const uint32_t v = ordered_bits(f[c]);
+            lo[c] = min(lo[c], v);
+            hi[c] = max(hi[c], v);
+        }
+    }
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        for (int o = 16; o > 0; o >>= 1) {
+            lo[c] = min(lo[c], __shfl_xor_sync(0xffffffffu, lo[c], o));
+            hi[c] = max(hi[c], __shfl_xor_sync(0xffffffffu, hi[c], o));
+        }
+        if ((threadIdx.x & 31u) == 0u) {
+            atomicMin(bounds6 + c, lo[c]);
+            atomicMax(bounds6 + 3 + c, hi[c]);
+        }
+    }
+}
+
+__device__ __forceinline__ uint64_t spread21(uint32_t v) {  // bit b -> bit 3b
+    uint64_t x = v & 0x1FFFFFu;
+    x = (x | (x << 32)) & 0x1F00000000FFFFull;
+    x = (x | (x << 16)) & 0x1F0000FF0000FFull;
+    x = (x | (x << 8)) & 0x100F00F00F00F00Full;
+    x = (x | (x << 4)) & 0x10C30C30C30C30C3ull;
+    x = (x | (x << 2)) & 0x1249249249249249ull;
+    return x;
+}
+
+__global__ void __launch_bounds__(256) morton_keys_kernel(const float4* __restrict__ pos, uint32_t n,
+                                                          const uint32_t* __restrict__ bounds6,
+                                                          unsigned long long* __restrict__ keys,
+                                                          uint32_t* __restrict__ index) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float4 p = __ldg(pos + i);
+    const float v[3] = {p.x, p.y, p.z};
+    uint32_t q[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        const float mn = from_ordered_bits(bounds6[c]), mx = from_ordered_bits(bounds6[3 + c]);
+        const float den = __fsub_rn(mx, mn), num = __fsub_rn(v[c], mn);
+        const float rel = den != 0.0f ? __fdiv_rn(num, den) : 0.0f;
+        q[c] = (uint32_t)__float2int_rz(__fmul_rn(rel, (float)((1 << 21) - 1)));
+    }
+    keys[i] = spread21(q[0]) | (spread21(q[1]) << 1) | (spread21(q[2]) << 2);
+    index[i] = i;
+}
+
+template <class T>
+__global__ void __launch_bounds__(256) gather_kernel(const T* __restrict__ src, const uint32_t* __restrict__ order,
+                                                     uint32_t n, uint32_t per, T* __restrict__ dst) {
+    const uint64_t total = (uint64_t)n * per;
+    for (uint64_t j = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; j < total; j += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t i = j / per, k = j - i * per;
+        dst[j] = __ldg(src + (uint64_t)__ldg(order + i) * per + k);
+    }
+}
+
+}  // namespace
+
+cudaError_t morton_order_device(const float4* pos, uint32_t n, uint32_t* order, cudaStream_t st) {
+    if (n == 0) return cudaSuccess;
+    uint32_t* bounds6 = nullptr;
+    unsigned long long *keys = nullptr, *keys_out = nullptr;
+    uint32_t* index = nullptr;
+    void* temp = nullptr;
+    size_t temp_bytes = 0;
+    const uint32_t init[6] = {0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu, 0u, 0u, 0u};
+    cudaError_t e = cudaMalloc(&bounds6, 6 * sizeof(uint32_t));
+    if (e == cudaSuccess) e = cudaMalloc(&keys, (size_t)n * 8);
+    if (e == cudaSuccess) e = cudaMalloc(&keys_out, (size_t)n * 8);
+    if (e == cudaSuccess) e = cudaMalloc(&index, (size_t)n * 4);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(bounds6, init, sizeof(init), cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) {
+        mean_bounds_kernel<<<148 * 8, 256, 0, st>>>(pos, n, bounds6);
+        morton_keys_kernel<<<(n + 255) / 256, 256, 0, st>>>(pos, n, bounds6, keys, index);
+        e = cudaGetLastError();
+    }
+    // 63 key bits; the radix sort is stable, so equal keys keep their input order as the
+    // host's std::stable_sort does
+    if (e == cudaSuccess) e = cub::DeviceRadixSort::SortPairs(nullptr, temp_bytes, keys, keys_out, index, order, (int)n, 0, 63, st);
+    if (e == cudaSuccess) e = cudaMalloc(&temp, temp_bytes);
+    if (e == cudaSuccess) e = cub::DeviceRadixSort::SortPairs(temp, temp_bytes, keys, keys_out, index, order, (int)n, 0, 63, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    cudaFree(temp);
+    cudaFree(index);
+    cudaFree(keys_out);
+    cudaFree(keys);
+    cudaFree(bounds6);
+    return e;
+}
+
+void launch_gather_rows(const float4* src, const uint32_t* order, uint32_t n, uint32_t per, float4* dst, cudaStream_t st) {
+    if (n) gather_kernel<float4><<<148 * 8, 256, 0, st>>>(src, order, n, per, dst);
+}
+
+}  // namespace gps

@@ -49,7 +49,9 @@ struct PassCounters {
     uint32_t scan_timeouts;  // always 0: no device-side wait can give up
     uint32_t loaded;         // Gaussians whose attributes the pass's preprocess read (after the
                              // block cull and pass 2's previous-mask test); 0 without a tally
-    uint32_t pad[2];
+    uint32_t crowded;        // 1 if a screen bin held more than kBinCrowded survivors: the
+                             // pass is walked in Gaussian order
+    uint32_t pad;
 };
 
 struct FrameConst {
@@ -125,6 +127,7 @@ struct ScanArgs {
     uint32_t* sorted_gid;        // [n] survivors in bin order
     uint32_t* sorted_pstart;     //     their first points (reference point indices)
     uint32_t* sorted_qstart;     //     their first walk positions in bin order
+    uint32_t bin_crowded;        // survivors of one bin past which the pass keeps Gaussian order
 };
 
 struct SplatArgs {
@@ -155,6 +158,13 @@ struct SplatArgs {
 // the same time write a compact part of the buffer.  Only the order changes: every point keeps
 // its reference point index (its seed) and the min is order-free.
 constexpr uint32_t kMaxBins = 16384;  // screen bins per pass (bins widen beyond 8192 x 8192 pixels)
+#ifndef GPS_BIN_CROWDED
+#define GPS_BIN_CROWDED 131072
+#endif
+// Survivors of one bin past which binning costs more than it saves: each takes its place with
+// an atomic on the bin's cursor, and those serialise (about 1.7 ns each).  The environment
+// variable GPS_BIN_CROWDED overrides it when a renderer is created.
+constexpr uint32_t kBinCrowded = GPS_BIN_CROWDED;
 #ifndef GPS_SPLAT_BINNED
 #define GPS_SPLAT_BINNED 1
 #endif
@@ -210,6 +220,13 @@ void launch_resolve(const ResolveArgs& a, bool depth_only, cudaStream_t stream);
 void launch_hiz_build(const HizView& h, const float* depth, int min_levels, cudaStream_t stream);
 void launch_block_bounds(const float4* pos_op, const float4* rot, const float4* scale, uint32_t n,
                          uint32_t per_block, float4* nodes, cudaStream_t stream);
+// Scene order on the device: order[j] = the input index of the j-th Gaussian in 3D Morton order
+// of the means, the order the host reorder (morton_sort) gives, key for key and tie for tie.
+// Allocates its own scratch; synchronizes the stream.
+cudaError_t morton_order_device(const float4* pos_op, uint32_t n, uint32_t* order, cudaStream_t stream);
+// dst[j * per + k] = src[order[j] * per + k]
+void launch_gather_rows(const float4* src, const uint32_t* order, uint32_t n, uint32_t per, float4* dst,
+                        cudaStream_t stream);
 void launch_taa(uint8_t* image, float* out_color, const float* cur_color, const float* prev_color,
                 const float* cur_depth, const float* prev_depth, const mat4& reproj, float blend, int width, int height,
                 int frame_number, cudaStream_t stream);

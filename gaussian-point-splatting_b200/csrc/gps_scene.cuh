@@ -14,7 +14,6 @@
 #pragma once
 #include <cstdint>
 #include <cuda_fp16.h>
-#include <cuda_fp8.h>
 #include <cuda_runtime.h>
 #include "gps_math.cuh"
 
@@ -258,12 +257,17 @@ struct SceneCompressed {
 
 // Half-precision storage (this library's own format, no counterpart in the reference), 80 bytes
 // per Gaussian, decoded to FP32 for all arithmetic:
-//   rec   uint4 : FP16 position relative to its block origin (x, y, z), FP16 opacity,
-//                 FP16 rotation (w, x, y, z)
-//   scl   uint4 : FP16 scale (x, y, z), FP16 SH DC term (r, g, b), FP32 AC scale k
-//   ac    3 x uint4 : the 45 AC SH coefficients (FP32 layout order 3..47) as FP8 e4m3 of
-//                 value / k, k = max |AC| / 448; 3 pad bytes
-//   origin float4 per kHalfOriginBlock Gaussians: the block's position origin
+//   rec   uint4 : position as 16-bit fixed-point offsets (x, y, z) from its block origin in
+//                 steps of the origin's w, FP16 opacity, FP16 rotation (w, x, y, z)
+//   scl   uint4 : FP16 scale (x, y, z), FP16 SH DC term (r, g, b), bf16 AC scales k1, k2
+//   ac    3 x uint4 : the 45 AC SH coefficients (FP32 layout order 3..47) as int8 q with
+//                 value = q * k_band (band 1: AC 0-8, band 2: 9-23, band 3: 24-44;
+//                 k_band = max |AC of the band| / 127, rounded up to bf16); bytes 45-46 hold
+//                 k3, byte 47 is zero
+//   origin float4 per kHalfOriginBlock Gaussians: the centre of the block's means and the step
+//                 w = largest half-extent / 32767 (16 bits over the block's extent, where
+//                 FP16 offsets keep 11; the offsets' rounding moved thin coplanar Gaussians
+//                 in front of one another)
 // The DC term carries most of a Gaussian's colour, so it keeps 11 significant bits.
 constexpr uint32_t kHalfOriginBlock = 16;
 
@@ -285,7 +289,8 @@ struct SceneHalf {
         const uint4 r = __ldg(&rec[g]);
         const uint4 c = __ldg(&scl[g]);
         const float4 o = __ldg(&origin[g / kHalfOriginBlock]);
-        mean = make_v3(o.x + h(r.x, 0), o.y + h(r.x, 1), o.z + h(r.y, 0));
+        mean = make_v3(o.x + (float)(int16_t)(r.x & 0xFFFFu) * o.w, o.y + (float)(int16_t)(r.x >> 16) * o.w,
+                       o.z + (float)(int16_t)(r.y & 0xFFFFu) * o.w);
         quat = make_v4(h(r.z, 0), h(r.z, 1), h(r.w, 0), h(r.w, 1));
         s = make_v3(h(c.x, 0), h(c.x, 1), h(c.y, 0));
     }
@@ -295,20 +300,15 @@ struct SceneHalf {
         shs_[0] = h(c.y, 1);
         shs_[1] = h(c.z, 0);
         shs_[2] = h(c.z, 1);
-        const float k = __uint_as_float(c.w);
         const uint4* src = ac + (size_t)g * 3;
+        const uint4 a0 = __ldg(&src[0]), a1 = __ldg(&src[1]), a2 = __ldg(&src[2]);
+        const uint32_t w[12] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w, a2.x, a2.y, a2.z, a2.w};
+        const float k1 = __uint_as_float(c.w << 16), k2 = __uint_as_float(c.w & 0xFFFF0000u);
+        const float k3 = __uint_as_float((w[11] << 8) & 0xFFFF0000u);
 #pragma unroll
-        for (int i = 0; i < 3; ++i) {
-            const uint4 v = __ldg(&src[i]);
-            const uint32_t w[4] = {v.x, v.y, v.z, v.w};
-#pragma unroll
-            for (int j = 0; j < 16; ++j) {
-                const int e = 16 * i + j;
-                if (e >= 45) break;
-                __nv_fp8_e4m3 q;
-                q.__x = (__nv_fp8_storage_t)((w[j >> 2] >> (8 * (j & 3))) & 0xFFu);
-                shs_[3 + e] = (float)q * k;
-            }
+        for (int e = 0; e < 45; ++e) {
+            const int q = (int)(int8_t)((w[e >> 2] >> (8 * (e & 3))) & 0xFFu);
+            shs_[3 + e] = (float)q * (e < 9 ? k1 : (e < 24 ? k2 : k3));
         }
         return color_from_sh_fp32(mean, campos, shs_);
     }

@@ -5,6 +5,7 @@
 // the values handed to the kernels are bit-identical to the reference's.
 #pragma once
 #include <cstdint>
+#include <functional>
 #include <string>
 #include <vector>
 #include "gps_math.cuh"
@@ -22,6 +23,10 @@ struct CpuGaussian {
 };
 static_assert(sizeof(CpuGaussian) == 236, "CpuGaussian must match the reference layout");
 
+// ---- host threads ------------------------------------------------------------------
+// f(begin, end) over [0, n) split across the host's cores (one range below 65,536 items).
+void parallel_ranges(uint64_t n, const std::function<void(uint64_t, uint64_t)>& f);
+
 // ---- errors ------------------------------------------------------------------------
 void set_last_error(const std::string& msg);
 const char* last_error();
@@ -29,6 +34,12 @@ const char* last_error();
 // ---- PLY (gaussian_loader.cu:115-245,282-427,480-562, ply_comments.h) ---------------
 // Returns 0 on success, otherwise a gps_status value (see include/gps_b200.h).
 int ply_read(const std::string& path, std::vector<CpuGaussian>& out, std::vector<std::string>& comments);
+// The vertex count and comments from the header alone.
+int ply_count(const std::string& path, uint64_t& count, std::vector<std::string>& comments);
+// Reads into caller memory of `capacity` Gaussians (the next chunk is read while the current one
+// is converted); count receives the vertex count.
+int ply_read_into(const std::string& path, CpuGaussian* out, uint64_t capacity, uint64_t& count,
+                  std::vector<std::string>& comments);
 int ply_write(const std::string& path, const CpuGaussian* g, uint64_t n, const std::vector<std::string>& comments);
 bool has_bvh_sorted_comment(const std::vector<std::string>& comments);
 // 3DGS output directory -> point_cloud/<alphabetically last>/point_cloud.ply
@@ -36,6 +47,8 @@ bool has_bvh_sorted_comment(const std::vector<std::string>& comments);
 int resolve_model_path(const std::string& in, std::string& out);
 // --sort-morton-order reorder (gaussian_loader.cu:363-424)
 void morton_sort(std::vector<CpuGaussian>& g);
+// The permutation morton_sort applies: order[j] = the input index of the j-th Gaussian.
+void morton_order(const CpuGaussian* g, uint64_t n, uint32_t* order);
 
 // ---- compressed scene encoding (gaussian_types.cuh:127-320, sh.cuh:28-39) ------------
 SceneBounds compute_scene_bounds(const CpuGaussian* g, uint64_t n);

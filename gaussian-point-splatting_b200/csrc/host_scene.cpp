@@ -13,6 +13,7 @@
 #include <cstring>
 #include <filesystem>
 #include <fstream>
+#include <functional>
 #include <numeric>
 #include <sstream>
 #include <thread>
@@ -25,6 +26,7 @@ thread_local std::string g_last_error;
 
 constexpr int kStatusIo = 2;
 constexpr int kStatusFormat = 3;
+constexpr int kStatusSize = 6;
 
 float sigmoid_ref(float x) {
     float v = 1.0f / (1.0f + std::exp(-x));
@@ -96,6 +98,12 @@ void parallel_for(uint64_t n, F f) {
     for (auto& t : ts) t.join();
 }
 
+}  // namespace
+
+void parallel_ranges(uint64_t n, const std::function<void(uint64_t, uint64_t)>& f) { parallel_for(n, f); }
+
+namespace {
+
 uint64_t morton3d21(int x, int y, int z) {
     uint64_t code = 0;
     for (int bit = 0; bit < 21; ++bit) {
@@ -160,15 +168,13 @@ int resolve_model_path(const std::string& in, std::string& out) {
     return 0;
 }
 
-int ply_read(const std::string& path, std::vector<CpuGaussian>& out, std::vector<std::string>& comments) {
-    std::ifstream f(path, std::ios::binary);
-    if (!f.is_open()) {
-        set_last_error("failed to open file: " + path);
-        return kStatusIo;
-    }
+namespace {
+
+// The header of a binary little-endian 3DGS PLY: property offsets, vertex count, comments; the
+// stream is left at the first record.  Returns 0 or a gps_status value.
+int ply_header(std::ifstream& f, const std::string& path, Offsets& o, size_t& count, std::vector<std::string>& comments) {
     comments.clear();
-    Offsets o;
-    size_t count = 0;
+    count = 0;
     size_t off = 0;
     bool in_vertex = false, saw_end = false, saw_magic = false, binary_le = false;
     std::string line;
@@ -243,18 +249,83 @@ int ply_read(const std::string& path, std::vector<CpuGaussian>& out, std::vector
     for (size_t i = 0; i < o.rest.size() && i < 45; ++i)
         if (o.rest.size() >= 45 && o.rest[i] == kMissing) { set_last_error("f_rest fields are not contiguous"); return kStatusFormat; }
 
-    const size_t need = count * o.record;
-    std::vector<uint8_t> buf(need);
-    f.read(reinterpret_cast<char*>(buf.data()), (std::streamsize)need);
-    if ((size_t)f.gcount() != need) {
-        set_last_error("short read: expected " + std::to_string(count) + " records in " + path);
+    return 0;
+}
+
+int ply_open(const std::string& path, std::ifstream& f) {
+    f.open(path, std::ios::binary);
+    if (!f.is_open()) {
+        set_last_error("failed to open file: " + path);
         return kStatusIo;
     }
-    out.resize(count);
-    parallel_for(count, [&](uint64_t b, uint64_t e) {
-        for (uint64_t i = b; i < e; ++i) record_to_gaussian(buf.data() + i * o.record, o, out[i]);
-    });
     return 0;
+}
+
+}  // namespace
+
+int ply_count(const std::string& path, uint64_t& count, std::vector<std::string>& comments) {
+    std::ifstream f;
+    int rc = ply_open(path, f);
+    if (rc) return rc;
+    Offsets o;
+    size_t c = 0;
+    rc = ply_header(f, path, o, c, comments);
+    count = c;
+    return rc;
+}
+
+int ply_read_into(const std::string& path, CpuGaussian* out, uint64_t capacity, uint64_t& count,
+                  std::vector<std::string>& comments) {
+    std::ifstream f;
+    int rc = ply_open(path, f);
+    if (rc) return rc;
+    Offsets o;
+    size_t c = 0;
+    rc = ply_header(f, path, o, c, comments);
+    if (rc) return rc;
+    count = c;
+    if (capacity < c) {
+        set_last_error("output capacity too small");
+        return kStatusSize;
+    }
+    // records in 64 MiB chunks: the next chunk is read while the current one is converted on
+    // every core
+    const size_t per = std::max<size_t>(1, ((size_t)64 << 20) / o.record);
+    std::vector<uint8_t> buf[2];
+    auto read_chunk = [&](size_t b, std::vector<uint8_t>& into) -> bool {
+        const size_t m = std::min(per, c - b);
+        into.resize(m * o.record);
+        f.read(reinterpret_cast<char*>(into.data()), (std::streamsize)into.size());
+        return (size_t)f.gcount() == into.size();
+    };
+    if (!read_chunk(0, buf[0])) {
+        set_last_error("short read: expected " + std::to_string(c) + " records in " + path);
+        return kStatusIo;
+    }
+    for (size_t b = 0, k = 0; b < c; b += per, k ^= 1) {
+        const size_t m = std::min(per, c - b);
+        bool next_ok = true;
+        std::thread reader;
+        if (b + per < c) reader = std::thread([&, b, k]() { next_ok = read_chunk(b + per, buf[k ^ 1]); });
+        const uint8_t* src = buf[k].data();
+        parallel_for(m, [&](uint64_t lo, uint64_t hi) {
+            for (uint64_t i = lo; i < hi; ++i) record_to_gaussian(src + i * o.record, o, out[b + i]);
+        });
+        if (reader.joinable()) reader.join();
+        if (!next_ok) {
+            set_last_error("short read: expected " + std::to_string(c) + " records in " + path);
+            return kStatusIo;
+        }
+    }
+    return 0;
+}
+
+int ply_read(const std::string& path, std::vector<CpuGaussian>& out, std::vector<std::string>& comments) {
+    uint64_t count = 0;
+    int rc = ply_count(path, count, comments);
+    if (rc) return rc;
+    out.resize(count);
+    return ply_read_into(path, out.data(), count, count, comments);
 }
 
 int ply_write(const std::string& path, const CpuGaussian* g, uint64_t n, const std::vector<std::string>& comments) {
@@ -306,11 +377,11 @@ int ply_write(const std::string& path, const CpuGaussian* g, uint64_t n, const s
     return 0;
 }
 
-void morton_sort(std::vector<CpuGaussian>& g) {
-    const size_t n = g.size();
+void morton_order(const CpuGaussian* g, uint64_t n, uint32_t* order) {
     if (n == 0) return;
     vec3 mn = make_v3(FLT_MAX, FLT_MAX, FLT_MAX), mx = make_v3(-FLT_MAX, -FLT_MAX, -FLT_MAX);
-    for (auto& q : g) {
+    for (uint64_t i = 0; i < n; ++i) {
+        const CpuGaussian& q = g[i];
         mn = make_v3(gmin(mn.x, q.mean[0]), gmin(mn.y, q.mean[1]), gmin(mn.z, q.mean[2]));
         mx = make_v3(gmax(mx.x, q.mean[0]), gmax(mx.y, q.mean[1]), gmax(mx.z, q.mean[2]));
     }
@@ -324,9 +395,15 @@ void morton_sort(std::vector<CpuGaussian>& g) {
             key[i] = morton3d21((int)(rel[0] * s), (int)(rel[1] * s), (int)(rel[2] * s));
         }
     });
+    std::iota(order, order + n, 0u);
+    std::stable_sort(order, order + n, [&](uint32_t a, uint32_t b) { return key[a] < key[b]; });
+}
+
+void morton_sort(std::vector<CpuGaussian>& g) {
+    const size_t n = g.size();
+    if (n == 0) return;
     std::vector<uint32_t> idx(n);
-    std::iota(idx.begin(), idx.end(), 0u);
-    std::stable_sort(idx.begin(), idx.end(), [&](uint32_t a, uint32_t b) { return key[a] < key[b]; });
+    morton_order(g.data(), n, idx.data());
     std::vector<CpuGaussian> tmp(n);
     for (size_t j = 0; j < n; ++j) tmp[j] = g[idx[j]];
     g.swap(tmp);

@@ -9,6 +9,7 @@
 // a fixed sequence of asynchronous launches on the caller's stream.
 #include <algorithm>
 #include <cstdio>
+#include <cstdlib>
 #include <thread>
 #include <deque>
 #include <condition_variable>
@@ -108,15 +109,52 @@ struct gps_scene {
 
 namespace {
 
-void scene_upload(gps_scene* s, const CpuGaussian* g, uint64_t n) {
+void check_order(cudaError_t e) {
+    if (e == cudaErrorMemoryAllocation) {
+        cudaGetLastError();
+        throw CudaError(std::string("cudaMalloc in the device Morton reorder: ") + cudaGetErrorString(e));
+    }
+    if (e != cudaSuccess) throw CudaError(std::string("device Morton reorder: ") + cudaGetErrorString(e));
+}
+
+// The Morton order of host Gaussians computed on the device (only the means travel).
+void device_morton_order(const CpuGaussian* g, uint64_t n, uint32_t* order_host) {
+    if (n == 0) return;
+    std::vector<float4> pos(n);
+    for (uint64_t i = 0; i < n; ++i) pos[i] = make_float4(g[i].mean[0], g[i].mean[1], g[i].mean[2], 0.0f);
+    dptr<float4> d_pos(dev_alloc<float4>(n));
+    dptr<uint32_t> d_order(dev_alloc<uint32_t>(n));
+    GPS_CUDA(cudaMemcpy(d_pos.get(), pos.data(), n * sizeof(float4), cudaMemcpyHostToDevice));
+    check_order(morton_order_device(d_pos.get(), (uint32_t)n, d_order.get(), 0));
+    GPS_CUDA(cudaMemcpy(order_host, d_order.get(), n * sizeof(uint32_t), cudaMemcpyDeviceToHost));
+}
+
+// device_sort: put the uploaded Gaussians in Morton order on the device (FP32 and HALF
+// scenes; the same order as morton_sort on the host).
+void scene_upload(gps_scene* s, const CpuGaussian* g, uint64_t n, bool device_sort) {
     s->n = n;
     s->per_block = gaussians_per_block(n);
     s->block_count = (uint32_t)((n + s->per_block - 1) / s->per_block);
-    // repack into 16-byte SoA in chunks through pinned staging
-    const uint64_t chunk = 1u << 20;
+    // repack into 16-byte SoA in chunks through two pinned staging halves: a chunk is repacked on
+    // every host core while the previous one is copied
+    const uint64_t chunk = 1u << 19;
     float4* stage = nullptr;
-    GPS_CUDA(cudaMallocHost(&stage, chunk * sizeof(float4) * 15));
+    GPS_CUDA(cudaMallocHost(&stage, 2 * chunk * sizeof(float4) * 15));
     std::unique_ptr<float4, void (*)(float4*)> stage_guard(stage, [](float4* p) { cudaFreeHost(p); });
+    cudaStream_t cs = nullptr;
+    cudaEvent_t ev[2] = {nullptr, nullptr};
+    GPS_CUDA(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+    struct CopyState {
+        cudaStream_t s;
+        cudaEvent_t* e;
+        ~CopyState() {
+            if (s) cudaStreamSynchronize(s);
+            for (int i = 0; i < 2; ++i)
+                if (e[i]) cudaEventDestroy(e[i]);
+            if (s) cudaStreamDestroy(s);
+        }
+    } copy_state{cs, ev};
+    for (int i = 0; i < 2; ++i) GPS_CUDA(cudaEventCreateWithFlags(&ev[i], cudaEventDisableTiming));
     float4* d_pos = dev_alloc<float4>(n);
     s->pos_op.reset(d_pos);
     float4* d_rot = dev_alloc<float4>(n);
@@ -128,23 +166,50 @@ void scene_upload(gps_scene* s, const CpuGaussian* g, uint64_t n) {
         d_sh = dev_alloc<float4>(n * 12);
         s->sh.reset(d_sh);
     }
-    for (uint64_t b = 0; b < n; b += chunk) {
-        uint64_t e = std::min(n, b + chunk), m = e - b;
-        float4* sp = stage;
-        float4* sr = stage + chunk;
-        float4* ss = stage + 2 * chunk;
-        float4* sh = stage + 3 * chunk;
-        for (uint64_t i = 0; i < m; ++i) {
-            const CpuGaussian& q = g[b + i];
-            sp[i] = make_float4(q.mean[0], q.mean[1], q.mean[2], q.opacity);
-            sr[i] = make_float4(q.rot[0], q.rot[1], q.rot[2], q.rot[3]);
-            ss[i] = make_float4(q.scale[0], q.scale[1], q.scale[2], 0.0f);
-            if (d_sh) std::memcpy(sh + i * 12, q.sh, sizeof(float) * 48);
-        }
-        GPS_CUDA(cudaMemcpy(d_pos + b, sp, m * sizeof(float4), cudaMemcpyHostToDevice));
-        GPS_CUDA(cudaMemcpy(d_rot + b, sr, m * sizeof(float4), cudaMemcpyHostToDevice));
-        GPS_CUDA(cudaMemcpy(d_scale + b, ss, m * sizeof(float4), cudaMemcpyHostToDevice));
-        if (d_sh) GPS_CUDA(cudaMemcpy(d_sh + b * 12, sh, m * 12 * sizeof(float4), cudaMemcpyHostToDevice));
+    uint64_t k = 0;
+    for (uint64_t b = 0; b < n; b += chunk, ++k) {
+        const uint64_t e = std::min(n, b + chunk), m = e - b;
+        float4* buf = stage + (k & 1) * chunk * 15;
+        if (k >= 2) GPS_CUDA(cudaEventSynchronize(ev[k & 1]));  // its previous copy is done
+        float4* sp = buf;
+        float4* sr = buf + chunk;
+        float4* ss = buf + 2 * chunk;
+        float4* sh = buf + 3 * chunk;
+        const bool with_sh = d_sh != nullptr;
+        parallel_ranges(m, [&](uint64_t lo, uint64_t hi) {
+            for (uint64_t i = lo; i < hi; ++i) {
+                const CpuGaussian& q = g[b + i];
+                sp[i] = make_float4(q.mean[0], q.mean[1], q.mean[2], q.opacity);
+                sr[i] = make_float4(q.rot[0], q.rot[1], q.rot[2], q.rot[3]);
+                ss[i] = make_float4(q.scale[0], q.scale[1], q.scale[2], 0.0f);
+                if (with_sh) std::memcpy(sh + i * 12, q.sh, sizeof(float) * 48);
+            }
+        });
+        GPS_CUDA(cudaMemcpyAsync(d_pos + b, sp, m * sizeof(float4), cudaMemcpyHostToDevice, cs));
+        GPS_CUDA(cudaMemcpyAsync(d_rot + b, sr, m * sizeof(float4), cudaMemcpyHostToDevice, cs));
+        GPS_CUDA(cudaMemcpyAsync(d_scale + b, ss, m * sizeof(float4), cudaMemcpyHostToDevice, cs));
+        if (d_sh) GPS_CUDA(cudaMemcpyAsync(d_sh + b * 12, sh, m * 12 * sizeof(float4), cudaMemcpyHostToDevice, cs));
+        GPS_CUDA(cudaEventRecord(ev[k & 1], cs));
+    }
+    GPS_CUDA(cudaStreamSynchronize(cs));
+    if (device_sort && n > 1) {
+        dptr<uint32_t> order(dev_alloc<uint32_t>(n));
+        check_order(morton_order_device(d_pos, (uint32_t)n, order.get(), 0));
+        auto regather = [&](dptr<float4>& arr, uint32_t per) {
+            float4* dst = dev_alloc<float4>(n * per);
+            launch_gather_rows(arr.get(), order.get(), (uint32_t)n, per, dst, 0);
+            GPS_CUDA(cudaGetLastError());
+            GPS_CUDA(cudaDeviceSynchronize());
+            arr.reset(dst);
+        };
+        regather(s->pos_op, 1);
+        regather(s->rot, 1);
+        regather(s->scale, 1);
+        if (d_sh) regather(s->sh, 12);
+        d_pos = s->pos_op.get();
+        d_rot = s->rot.get();
+        d_scale = s->scale.get();
+        d_sh = s->sh.get();
     }
     float4* nodes = dev_alloc<float4>((size_t)s->block_count * 2);
     s->block_nodes.reset(nodes);
@@ -249,6 +314,7 @@ struct gps_renderer {
     dptr<unsigned long long> tile_state;
     dptr<unsigned long long> bins;  // screen-bin histogram / cursors, kMaxBins + 1 words
     dptr<uint32_t> sorted_gid, sorted_pstart, sorted_qstart;  // survivors in screen-bin order
+    uint32_t bin_crowded = kBinCrowded;  // see kBinCrowded
     dptr<PassCounters> counters;  // [2]: pass 1, pass 2
     dptr<float> mip;
     dptr<unsigned> hiz_done;
@@ -419,6 +485,7 @@ void render_pass(gps_renderer* r, const FrameConst& fc, int frame, bool first, c
     sa.counters = pc;
     sa.loaded = r->loaded.get();
     sa.bins = binned ? r->bins.get() : nullptr;
+    sa.bin_crowded = r->bin_crowded;
     sa.nbins = nbins;
     sa.bin_shift = bin_shift;
     sa.bins_x = bins_x;
@@ -546,7 +613,9 @@ gps_status gps_settings_parse_args(int32_t argc, const char* const* argv, gps_se
     return GPS_OK;
 }
 
-static gps_status scene_create(std::vector<CpuGaussian>& g, int32_t format, bool presorted, gps_scene** out) {
+// sort: 0 keeps the given order, 1 reorders on the host (morton_sort), 2 on the device.
+static gps_status scene_create(std::vector<CpuGaussian>& g, int32_t format, bool presorted, gps_scene** out,
+                               int32_t sort = 0) {
     if (format != GPS_SCENE_FP32 && format != GPS_SCENE_COMPRESSED && format != GPS_SCENE_HALF)
         return fail(GPS_ERR_INVALID_ARGUMENT, "unknown scene format");
     if (g.size() >= (1ull << 30)) return fail(GPS_ERR_SIZE, "scenes are limited to 2^30 Gaussians");
@@ -554,7 +623,18 @@ static gps_status scene_create(std::vector<CpuGaussian>& g, int32_t format, bool
     s->format = format;
     s->presorted = presorted;
     try {
-        scene_upload(s.get(), g.data(), g.size());
+        if (sort == 1) morton_sort(g);
+        bool device_sort = sort == 2;
+        if (device_sort && format == GPS_SCENE_COMPRESSED) {
+            // the compressed encoding is made on the host: order the host copy by the device's keys
+            std::vector<uint32_t> order(g.size());
+            device_morton_order(g.data(), g.size(), order.data());
+            std::vector<CpuGaussian> tmp(g.size());
+            for (size_t j = 0; j < g.size(); ++j) tmp[j] = g[order[j]];
+            g.swap(tmp);
+            device_sort = false;
+        }
+        scene_upload(s.get(), g.data(), g.size(), device_sort);
     } catch (const CudaError& e) {
         return fail(std::string(e.what()).find("cudaMalloc") != std::string::npos ? GPS_ERR_OUT_OF_MEMORY : GPS_ERR_CUDA, e.what());
     }
@@ -574,9 +654,9 @@ gps_status gps_scene_load_ply(const char* path, int32_t format, int32_t sort_mor
     rc = ply_read(resolved, g, comments);
     if (rc) return (gps_status)rc;
     bool presorted = has_bvh_sorted_comment(comments);
-    if (sort_morton_order && !presorted) morton_sort(g);
     if (presorted_out) *presorted_out = presorted ? 1 : 0;
-    return scene_create(g, format, presorted, out);
+    // a file written in BVH order keeps it (gaussian_loader.cu:363)
+    return scene_create(g, format, presorted, out, presorted ? 0 : (sort_morton_order == 2 ? 2 : sort_morton_order ? 1 : 0));
 }
 
 gps_status gps_scene_from_host(const float* gaussians, uint64_t count, int32_t format, int32_t presorted,
@@ -586,6 +666,32 @@ gps_status gps_scene_from_host(const float* gaussians, uint64_t count, int32_t f
     std::vector<CpuGaussian> g(count);
     if (count) std::memcpy(g.data(), gaussians, count * sizeof(CpuGaussian));
     return scene_create(g, format, presorted != 0, out);
+}
+
+gps_status gps_scene_from_host_sorted(const float* gaussians, uint64_t count, int32_t format, int32_t sort_morton_order,
+                                      gps_scene** out) {
+    if (!out || (!gaussians && count)) return fail(GPS_ERR_INVALID_ARGUMENT, "null argument");
+    if (sort_morton_order < 0 || sort_morton_order > 2) return fail(GPS_ERR_INVALID_ARGUMENT, "sort_morton_order must be 0, 1 or 2");
+    *out = nullptr;
+    std::vector<CpuGaussian> g(count);
+    if (count) std::memcpy(g.data(), gaussians, count * sizeof(CpuGaussian));
+    return scene_create(g, format, false, out, sort_morton_order);
+}
+
+gps_status gps_morton_order(const float* gaussians, uint64_t count, int32_t on_device, uint32_t* order) {
+    if ((!gaussians || !order) && count) return fail(GPS_ERR_INVALID_ARGUMENT, "null argument");
+    if (count >= (1ull << 30)) return fail(GPS_ERR_SIZE, "scenes are limited to 2^30 Gaussians");
+    const CpuGaussian* g = reinterpret_cast<const CpuGaussian*>(gaussians);
+    if (!on_device) {
+        morton_order(g, count, order);
+        return GPS_OK;
+    }
+    try {
+        device_morton_order(g, count, order);
+    } catch (const CudaError& e) {
+        return fail(std::string(e.what()).find("cudaMalloc") != std::string::npos ? GPS_ERR_OUT_OF_MEMORY : GPS_ERR_CUDA, e.what());
+    }
+    return GPS_OK;
 }
 
 uint64_t gps_scene_count(const gps_scene* scene) { return scene ? scene->n : 0; }
@@ -656,16 +762,13 @@ gps_status gps_ply_read(const char* path, float* out, uint64_t capacity, uint64_
     std::string resolved;
     int rc = resolve_model_path(path, resolved);
     if (rc) return (gps_status)rc;
-    std::vector<CpuGaussian> g;
     std::vector<std::string> comments;
-    rc = ply_read(resolved, g, comments);
+    uint64_t n = 0;
+    rc = out ? ply_read_into(resolved, reinterpret_cast<CpuGaussian*>(out), capacity, n, comments)
+             : ply_count(resolved, n, comments);  // count only: the header alone
+    *count = n;
     if (rc) return (gps_status)rc;
-    *count = g.size();
     if (presorted) *presorted = has_bvh_sorted_comment(comments) ? 1 : 0;
-    if (out) {
-        if (capacity < g.size()) return fail(GPS_ERR_SIZE, "output capacity too small");
-        std::memcpy(out, g.data(), g.size() * sizeof(CpuGaussian));
-    }
     return GPS_OK;
 }
 
@@ -740,6 +843,7 @@ gps_status create_renderer(gps_scene* scene, const gps_settings* settings, const
     r->scan_tiles = scan_tile_count(r->n);
     r->n_pad = r->scan_tiles * kScanTileGaussians;
     r->cap_entries = std::max(entries, cap_entries);
+    if (const char* v = std::getenv("GPS_BIN_CROWDED")) r->bin_crowded = (uint32_t)std::strtoul(v, nullptr, 10);
     try {
         r->buffer.reset(dev_alloc<uint64_t>(r->cap_entries));
         r->counts.reset(dev_alloc<uint32_t>(std::max<uint32_t>(r->n_pad, 16)));
@@ -758,6 +862,7 @@ gps_status create_renderer(gps_scene* scene, const gps_settings* settings, const
         r->sorted_pstart.reset(dev_alloc<uint32_t>(std::max<uint32_t>(r->n, 1)));
         r->sorted_qstart.reset(dev_alloc<uint32_t>(std::max<uint32_t>(r->n, 1)));
         r->bins.reset(dev_alloc<unsigned long long>(kMaxBins + 1));
+
         GPS_CUDA(cudaMemset(r->bins.get(), 0, sizeof(unsigned long long) * (kMaxBins + 1)));
         const uint64_t max_pts = (uint64_t)std::max(0, s.max_number_of_points);
         r->tile_first_rank.reset(dev_alloc<uint32_t>(max_pts / 256 + 2));
@@ -918,6 +1023,9 @@ gps_status gps_renderer_stats(gps_renderer* r, gps_stats* out) {
     out->kernel_launches = (int32_t)r->frame_launches;
     out->gaussians_read_one = (int32_t)c[0].loaded;
     out->gaussians_read_two = (int32_t)c[1].loaded;
+    const bool binned = GPS_SPLAT_BINNED != 0;
+    out->screen_order_one = (binned && c[0].points && !c[0].truncated && !c[0].crowded) ? 1 : 0;
+    out->screen_order_two = (binned && c[1].points && !c[1].truncated && !c[1].crowded) ? 1 : 0;
     if (out->device_timeouts) return fail(GPS_ERR_DEVICE_TIMEOUT, "a device-side look-back wait gave up");
     return GPS_OK;
 }

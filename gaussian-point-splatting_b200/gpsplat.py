@@ -129,6 +129,8 @@ class Stats(ctypes.Structure):
         ("kernel_launches", c_int32),
         ("gaussians_read_one", c_int32),
         ("gaussians_read_two", c_int32),
+        ("screen_order_one", c_int32),
+        ("screen_order_two", c_int32),
     ]
 
 
@@ -160,6 +162,8 @@ _SIGNATURES = [
     ("gps_settings_parse_args", c_int32, [c_int32, POINTER(c_char_p), POINTER(Settings), c_char_p, ctypes.c_size_t, c_char_p, ctypes.c_size_t]),
     ("gps_scene_load_ply", c_int32, [c_char_p, c_int32, c_int32, POINTER(c_void_p), POINTER(c_int32)]),
     ("gps_scene_from_host", c_int32, [c_void_p, c_uint64, c_int32, c_int32, POINTER(c_void_p)]),
+    ("gps_scene_from_host_sorted", c_int32, [c_void_p, c_uint64, c_int32, c_int32, POINTER(c_void_p)]),
+    ("gps_morton_order", c_int32, [c_void_p, c_uint64, c_int32, POINTER(c_uint32)]),
     ("gps_scene_tile", c_int32, [c_void_p, c_int32, POINTER(c_float), POINTER(c_void_p)]),
     ("gps_scene_count", c_uint64, [c_void_p]),
     ("gps_scene_format_of", c_int32, [c_void_p]),
@@ -329,6 +333,16 @@ class CameraPath:
             pass
 
 
+def morton_order(gaussians: np.ndarray, on_device: bool = False) -> np.ndarray:
+    """The Morton reorder's permutation (gps_morton_order): order[j] = input index of the j-th."""
+    g = np.ascontiguousarray(gaussians, dtype=np.float32)
+    assert g.ndim == 2 and g.shape[1] == GAUSSIAN_FLOATS
+    order = np.empty(g.shape[0], np.uint32)
+    _check(load_library().gps_morton_order(g.ctypes.data, g.shape[0], int(on_device),
+                                           order.ctypes.data_as(POINTER(c_uint32))))
+    return order
+
+
 class Scene:
     """Device-resident Gaussian scene (GPUGaussianScene*, gaussian_types.cuh:421-646)."""
 
@@ -337,7 +351,9 @@ class Scene:
         self.presorted = presorted
 
     @classmethod
-    def from_ply(cls, path: str, fmt: int = GPS_SCENE_FP32, sort_morton_order: bool = False) -> "Scene":
+    def from_ply(cls, path: str, fmt: int = GPS_SCENE_FP32, sort_morton_order: int = 0) -> "Scene":
+        """sort_morton_order: 0 file order, 1 Morton reorder on the host, 2 the same reorder on
+        the device (gaussian_loader.cu:363-424); a file in BVH order keeps its order."""
         h = c_void_p()
         pre = c_int32(0)
         _check(load_library().gps_scene_load_ply(path.encode(), fmt, int(sort_morton_order), byref(h), byref(pre)))
@@ -350,6 +366,15 @@ class Scene:
         h = c_void_p()
         _check(load_library().gps_scene_from_host(g.ctypes.data, g.shape[0], fmt, int(presorted), byref(h)))
         return cls(h, presorted)
+
+    @classmethod
+    def from_host_sorted(cls, gaussians: np.ndarray, fmt: int = GPS_SCENE_FP32, sort_morton_order: int = 2) -> "Scene":
+        """A scene in Morton order: 1 reorders on the host, 2 on the device (same order)."""
+        g = np.ascontiguousarray(gaussians, dtype=np.float32)
+        assert g.ndim == 2 and g.shape[1] == GAUSSIAN_FLOATS
+        h = c_void_p()
+        _check(load_library().gps_scene_from_host_sorted(g.ctypes.data, g.shape[0], fmt, int(sort_morton_order), byref(h)))
+        return cls(h, False)
 
     def tile(self, offsets_xz) -> "Scene":
         """A half-precision scene of translated copies of this one (gps_scene_tile)."""

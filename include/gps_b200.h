@@ -39,12 +39,11 @@ typedef enum gps_scene_format {
     GPS_SCENE_COMPRESSED = 1,  /* GPUGaussianSceneCompressed, the reference's default build
                                   (config.h:15, gaussian_types.cuh:421-541) */
     GPS_SCENE_HALF = 2         /* this library's own storage, no counterpart in the reference:
-                                  FP16 position (relative to a 16-Gaussian block origin), opacity,
-                                  rotation, scale and SH DC term, FP8 e4m3 SH AC terms with a
-                                  per-Gaussian FP32 scale; 80 bytes per Gaussian (FP32: 240),
-                                  decoded to FP32, near-degenerate 2D
-                                  covariances inverted in FP64.  Not bit-exact with the
-                                  reference by design. */
+                                  positions as 16-bit fixed-point offsets from a 16-Gaussian block
+                                  origin, FP16 opacity, rotation, scale and SH DC term, int8 SH
+                                  AC terms on one bf16 scale per SH band; 80 bytes per Gaussian
+                                  (FP32: 240), decoded to FP32, near-degenerate 2D covariances
+                                  inverted in FP64.  Not bit-exact with the reference by design. */
 } gps_scene_format;
 
 typedef enum gps_accumulation {
@@ -119,6 +118,10 @@ typedef struct gps_stats {
     int32_t gaussians_read_one, gaussians_read_two; /* Gaussians whose attributes the preprocess
                                                        read per pass (after the block cull and
                                                        pass 2's previous-mask test) */
+    int32_t screen_order_one, screen_order_two;     /* 1 if the pass's splat walked its survivors
+                                                       in screen-bin order, 0 in Gaussian order
+                                                       (budget-truncated pass, or a bin crowded
+                                                       past 131,072 survivors) */
 } gps_stats;
 
 typedef struct gps_scene gps_scene;
@@ -149,6 +152,17 @@ gps_status gps_scene_load_ply(const char* path, int32_t format, int32_t sort_mor
  * scale[3] (activated), rotation[4] (normalised, rot_0..rot_3). */
 gps_status gps_scene_from_host(const float* gaussians, uint64_t count, int32_t format,
                                int32_t presorted, gps_scene** out);
+/* gps_scene_from_host after the --sort-morton-order reorder (gaussian_loader.cu:363-424):
+ * sort_morton_order 0 keeps the given order, 1 reorders on the host, 2 on the device (keys,
+ * stable radix sort and gather in HBM).  1 and 2 give the identical order.  The same values
+ * select the reorder in gps_scene_load_ply, where a file carrying the bvh_sorted_order
+ * comment keeps its order. */
+gps_status gps_scene_from_host_sorted(const float* gaussians, uint64_t count, int32_t format,
+                                      int32_t sort_morton_order, gps_scene** out);
+/* The reorder's permutation: order[j] = the input index of the j-th Gaussian in 3D Morton
+ * order of the means (21 bits per axis over the means' bounding box, ties in input order);
+ * computed on the host (on_device = 0) or on the device. */
+gps_status gps_morton_order(const float* gaussians, uint64_t count, int32_t on_device, uint32_t* order);
 /* A new GPS_SCENE_HALF scene holding `copies` translated copies of a GPS_SCENE_HALF scene (copy
  * k moved by (offsets_xz[2k], 0, offsets_xz[2k+1])), built on the device; the culling blocks
  * follow the reference's size rule for the new count (like GaussianEditor::Repeat,

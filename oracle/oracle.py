@@ -214,3 +214,32 @@ def rgb36(rgb):
     out = np.zeros(rgb.shape[0], np.uint64)
     lib().oracle_rgb36(_p(rgb), rgb.shape[0], _p(out))
     return out
+
+
+def morton_order(gaussians: np.ndarray) -> np.ndarray:
+    """The --sort-morton-order permutation (gaussian_loader.cu:363-424): bounds of the means
+    (glm::min/max fold from FLT_MAX / -FLT_MAX, lines 365-377; a NaN never wins its
+    comparisons), rel = safe_div(mean - min, max - min) (lines 249-255, 387), 21-bit
+    truncation of rel * (2^21 - 1) (line 388), morton3D21 interleave x -> bit 3b, y -> 3b+1,
+    z -> 3b+2 (lines 257-265), then a stable sort of the keys (thrust::sort_by_key on uint64
+    keys, a radix sort, lines 397-404).  order[j] = the input index of the j-th Gaussian."""
+    g = np.asarray(gaussians, np.float32)
+    n = g.shape[0]
+    if n == 0:
+        return np.zeros(0, np.uint32)
+    mean = np.ascontiguousarray(g[:, 0:3], np.float32)
+    nan = np.isnan(mean)
+    fmax = np.float32(np.finfo(np.float32).max)
+    mn = np.minimum(np.where(nan, fmax, mean).min(axis=0), fmax).astype(np.float32)
+    mx = np.maximum(np.where(nan, -fmax, mean).max(axis=0), -fmax).astype(np.float32)
+    den = (mx - mn).astype(np.float32)
+    num = (mean - mn).astype(np.float32)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        rel = np.where(den != 0, num / np.where(den != 0, den, np.float32(1)), np.float32(0)).astype(np.float32)
+        scaled = (rel * np.float32((1 << 21) - 1)).astype(np.float32)
+        q = np.where(np.isfinite(scaled), scaled, 0).astype(np.int64) & 0x1FFFFF
+    key = np.zeros(n, np.uint64)
+    for bit in range(21):
+        for c in range(3):
+            key |= ((q[:, c].astype(np.uint64) >> np.uint64(bit)) & np.uint64(1)) << np.uint64(3 * bit + c)
+    return np.argsort(key, kind="stable").astype(np.uint32)

@@ -114,6 +114,8 @@ def harness_args(s, taa_race_free: bool = True) -> list[str]:
         a += ["--background"] + [repr(float(s.background[i])) for i in range(3)]
     if s.immediate_splat_threshold > 0:
         a += ["--immediate-threshold", str(s.immediate_splat_threshold)]
+    if s.sort_morton_order:
+        a.append("--sort-morton-order")
     if s.accumulation_mode == gpsplat.GPS_ACCUM_TAA:
         # the harness runs the reference's own temporalRender so that no pixel reads a
         # neighbour's blended value (its in-place blend otherwise races; see ref_harness.cu);
@@ -149,7 +151,7 @@ def run_reference(ply: str, settings, cams, variant="fp32", checksum_only=False,
                 d[name] = np.load(p)
         frames.append(d)
     extra = {}
-    for name in ("bvh_nodes", "bvh_gpb"):
+    for name in ("bvh_nodes", "bvh_gpb") + (("scene_cpu",) if settings.sort_morton_order else ()):
         p = os.path.join(out, f"{name}.npy")
         if os.path.exists(p):
             extra[name] = np.load(p)

@@ -95,6 +95,25 @@ def test_ply_roundtrip_and_activation(tmp_path):
     np.testing.assert_allclose(g2, g, rtol=2e-5, atol=2e-6)
 
 
+def test_ply_read_spans_chunks(tmp_path):
+    """The reader converts 64 MiB of records at a time while the next chunk is read: a file of
+    several chunks reads back like the activation of its fields, and one cut inside a later
+    chunk is a short read (GPS_ERR_IO)."""
+    raw = synth.cube(700_000, seed=6)  # 248-byte records: three chunks
+    p = str(tmp_path / "big.ply")
+    raw.write_ply(p)
+    g, _ = gpsplat.ply_read(p)
+    np.testing.assert_allclose(g, synth.activate(raw), rtol=1e-6, atol=1e-6)
+    assert np.array_equal(g[:, 0:3], raw.pos)
+    data = open(p, "rb").read()
+    cut = str(tmp_path / "cut.ply")
+    with open(cut, "wb") as f:
+        f.write(data[: len(data) - 200 * 248])
+    with pytest.raises(gpsplat.GpsError) as e:
+        gpsplat.ply_read(cut)
+    assert e.value.status == 2
+
+
 def test_ply_sh_rest_is_channel_major(tmp_path):
     raw = synth.town(300, seed=2)
     p = str(tmp_path / "town.ply")

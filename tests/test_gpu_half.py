@@ -1,7 +1,7 @@
 """The half-precision scene format (GPS_SCENE_HALF) and on-device tiling (gps_scene_tile).
 
-The format is this library's own (FP16 geometry and SH DC term, FP8 e4m3 SH AC terms with a
-per-Gaussian scale, FP64 inversion of near-degenerate 2D covariances), so it is not compared
+The format is this library's own (FP16 geometry and SH DC term, int8 SH AC terms on a per-band
+scale, FP64 inversion of near-degenerate 2D covariances), so it is not compared
 with the reference bit for bit.  Instead its converged image is compared with the FP32 path's:
 with the same sample streams the two must agree far better than two independent FP32
 estimates do, and against a long FP32 run its error may exceed the FP32 path's by a bounded
@@ -40,23 +40,26 @@ def _psnr(a, b):
     return 10.0 * np.log10(1.0 / np.mean((a - b) ** 2))
 
 
-def test_half_converges_like_fp32():
+@pytest.mark.parametrize("view", [3, 0, 5])
+def test_half_converges_like_fp32(view):
     ply = gpsutil.cached_ply("town60k", lambda: synth.town(60000, seed=5))
     s = gpsplat.default_settings(width=W, height=H, samples_per_pixel=4, max_number_of_points=4_000_000)
-    pose = synth.orbit(8, 30.0, 10.0)[3]
+    pose = synth.orbit(8, 30.0, 10.0)[view]
     f32 = gpsplat.Scene.from_ply(ply, gpsplat.GPS_SCENE_FP32)
     half = gpsplat.Scene.from_ply(ply, gpsplat.GPS_SCENE_HALF)
-    ref = _mean_image(f32, s, pose, 1000, 256)
-    a = _mean_image(f32, s, pose, 1, 32)
-    b = _mean_image(half, s, pose, 1, 32)
-    c = _mean_image(f32, s, pose, 5000, 32)
+    ref = _mean_image(f32, s, pose, 1000, 512)
+    a = _mean_image(f32, s, pose, 1, 64)
+    b = _mean_image(half, s, pose, 1, 64)
+    c = _mean_image(f32, s, pose, 5000, 64)
     same_seeds = _psnr(a, b)
     independent = _psnr(a, c)
     # the format's deviation is well below the sampling noise of an independent estimate
     assert same_seeds > independent + 2.0, (same_seeds, independent)
-    # and against the long FP32 run it costs at most 0.6 dB at 32 frames (measured about 0.3 dB
-    # at 64 frames of this view: FP8's three mantissa bits on the SH AC terms dominate)
-    assert _psnr(b, ref) > _psnr(a, ref) - 0.6, (_psnr(b, ref), _psnr(a, ref))
+    # against the long FP32 run the 64-frame mean loses at most 0.1 dB to the FP32 path's
+    # (`oracle/precision_study.py --half-budget`, this format's rounding emulated on the CPU
+    # oracle: 0.045, -0.017 and -0.020 dB on views 3, 0 and 5; with FP16 position offsets
+    # 0.159, 0.133 and 0.069 dB, and with FP8 AC terms as well 0.30, 0.29 and 0.22 dB)
+    assert _psnr(b, ref) > _psnr(a, ref) - 0.1, (_psnr(b, ref), _psnr(a, ref))
     f32.close()
     half.close()
 

@@ -81,18 +81,30 @@ CASES = {
     "c2_town2m_1080p": ("town2m", lambda: synth.town(2_000_000, seed=5), dict(width=1920, height=1080,
                         supersampling_factor=2, samples_per_pixel=4, accumulation_mode=gpsplat.GPS_ACCUM_TAA),
                         synth.orbit(3, 30.0, 10.0), "fp32", gpsplat.GPS_SCENE_FP32),
+    # the same with the Gaussian-order walk that a pass falls back to when a screen bin is crowded
+    "c2_town2m_crowded": ("town2m", lambda: synth.town(2_000_000, seed=5), dict(width=1920, height=1080,
+                          supersampling_factor=2, samples_per_pixel=4, accumulation_mode=gpsplat.GPS_ACCUM_TAA),
+                          synth.orbit(3, 30.0, 10.0), "fp32", gpsplat.GPS_SCENE_FP32),
 }
 
 # cases that must run the grouped splat walk in every pass of at least one frame
-GROUPED_MIN_POINTS = {"c1_cube1m": 1_300_000, "c2_town2m_1080p": 1_300_000}
+GROUPED_MIN_POINTS = {"c1_cube1m": 1_300_000, "c2_town2m_1080p": 1_300_000, "c2_town2m_crowded": 1_300_000}
 
 
 def _bits(words, n):
     return gpsutil.mask_bits(words, n)
 
 
+# the walk order each case must exercise in every frame's passes (1 = screen-bin order)
+SCREEN_ORDER = {"c2_town2m_1080p": 1, "c2_town2m_crowded": 0}
+
+
 @pytest.mark.parametrize("case", sorted(CASES))
-def test_reference_parity(case):
+def test_reference_parity(case, monkeypatch):
+    if case.endswith("_crowded"):
+        # every bin counts as crowded: the passes take the Gaussian-order walk that very large
+        # scenes (many survivors behind one screen bin) fall back to
+        monkeypatch.setenv("GPS_BIN_CROWDED", "0")
     scene_name, make, overrides, poses, variant, fmt = CASES[case]
     if gpsutil.ref_harness(variant) is None:
         pytest.skip("reference harness not built (oracle/ref/build_ref.sh)")
@@ -134,6 +146,11 @@ def test_reference_parity(case):
         passes = (int(st[0]), int(st[1])) if two_pass else (int(st[0]),)
         if case in GROUPED_MIN_POINTS and min(passes) >= GROUPED_MIN_POINTS[case]:
             grouped_frames += 1
+        so = m["stats_obj"]
+        if case in SCREEN_ORDER:
+            for order, pts in ((so.screen_order_one, so.num_points_one), (so.screen_order_two, so.num_points_two)):
+                if pts > 0 and order != SCREEN_ORDER[case]:
+                    problems.append(f"{tag}: walk order {order}, expected {SCREEN_ORDER[case]}")
         if m["stats_obj"].num_points_one != int(st[0]) or m["stats_obj"].num_points_two != int(st[1]):
             problems.append(f"{tag}: stats P1/P2 {m['stats_obj'].num_points_one}/{m['stats_obj'].num_points_two} vs {st[0]}/{st[1]}")
         valid = ml | (_bits(m["mask_other"], n) if two_pass else False)
