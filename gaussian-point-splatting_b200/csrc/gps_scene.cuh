@@ -128,6 +128,12 @@ GPS_D vec3 mix_sh(vec3 x, vec3 y, vec3 a) {
 
 #endif  // __CUDACC__
 
+#if defined(__CUDACC__)
+// Asks L2 for the line holding p (no register, no wait): the preprocess touches the next chunk's
+// attributes this way while it works on the current chunk.
+GPS_D void prefetch_l2(const void* p) { asm volatile("prefetch.global.L2 [%0];" ::"l"(p)); }
+#endif
+
 struct SceneFP32 {
     const float4* __restrict__ pos_op;
     const float4* __restrict__ rot;
@@ -139,6 +145,11 @@ struct SceneFP32 {
 #if defined(__CUDACC__)
     GPS_D float opacity(uint32_t g) const {
         return gmin(__ldg(&pos_op[g]).w, kMaxOpacity);
+    }
+    GPS_D void prefetch(uint32_t g) const {
+        prefetch_l2(pos_op + g);
+        prefetch_l2(rot + g);
+        prefetch_l2(scale + g);
     }
     GPS_D void geometry(uint32_t g, vec3& mean, vec4& quat, vec3& s) const {
         float4 a = __ldg(&pos_op[g]);
@@ -179,6 +190,10 @@ struct SceneCompressed {
 #if defined(__CUDACC__)
     GPS_D float opacity(uint32_t g) const {
         return gmin((float)__ldg(&opac[g]) / 255.0f, kMaxOpacity);
+    }
+    GPS_D void prefetch(uint32_t g) const {
+        prefetch_l2(geom + g);
+        if ((g & 31u) == 0u) prefetch_l2(opac + g);
     }
     // gaussian_types.cuh:322-374
     GPS_D void geometry(uint32_t g, vec3& mean, vec4& quat, vec3& s) const {
@@ -285,6 +300,10 @@ struct SceneHalf {
         return __half2float(__ushort_as_half((unsigned short)(hi ? (word >> 16) : (word & 0xFFFFu))));
     }
     GPS_D float opacity(uint32_t g) const { return gmin(h(__ldg(&rec[g]).y, 1), kMaxOpacity); }
+    GPS_D void prefetch(uint32_t g) const {
+        prefetch_l2(rec + g);
+        prefetch_l2(scl + g);
+    }
     GPS_D void geometry(uint32_t g, vec3& mean, vec4& quat, vec3& s) const {
         const uint4 r = __ldg(&rec[g]);
         const uint4 c = __ldg(&scl[g]);
