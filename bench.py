@@ -49,6 +49,9 @@ def workload_spec(name: str):
     if name == "town256m":  # the town tiled 4 x 4 in the half-precision format
         return dict(n=16_000_000, tiles=4, kind="town", fmt="half", width=1920, height=1080, ss=2, spp=4, reduce=1,
                     hier=1, occl=1, taa=1, frames=120)
+    if name == "town4m_tiled":  # profiling-size variant of town256m: the 4M town tiled 2 x 2 (16M)
+        return dict(n=4_000_000, tiles=2, kind="town", fmt="half", width=1920, height=1080, ss=2, spp=4, reduce=1,
+                    hier=1, occl=1, taa=1, frames=120)
     if name == "cube1m":
         return dict(n=1_000_000, kind="cube", width=640, height=360, ss=1, spp=1, reduce=1, hier=0, occl=0, taa=0,
                     frames=1)
@@ -705,7 +708,7 @@ def main():
     ap.add_argument("--steps", type=int, default=30)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="mine", choices=["mine", "reference"])
-    ap.add_argument("--workload", default="town16m", choices=["town16m", "town4m", "town256m", "cube1m", "batch64", "serve"])
+    ap.add_argument("--workload", default="town16m", choices=["town16m", "town4m", "town256m", "town4m_tiled", "cube1m", "batch64", "serve"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-reference-cuda", action="store_true", help="skip timing the reference's CUDA build")
     ap.add_argument("--quick-cpu", action="store_true", help="CPU baseline on all cores only (no 1-thread frame)")
