@@ -977,9 +977,6 @@ __device__ __forceinline__ void splat_point_unbiased_k(uint32_t point, const Spl
 constexpr int kSplatRounds = GPS_SPLAT_ROUNDS;
 constexpr int kSplatWindow = kSplatTile * kSplatRounds;
 
-#ifndef GPS_SPLAT_TILE_PREFETCH
-#define GPS_SPLAT_TILE_PREFETCH 0
-#endif
 // K > 0: unbiased splatting with K points per thread per pass; K = 0: any other setting.
 template <int K>
 #ifndef GPS_SPLAT_MIN_BLOCKS
@@ -1045,22 +1042,6 @@ __global__ void __launch_bounds__(kSplatTile, kSplatRounds > 1 ? (K >= 8 ? 2 : G
         constexpr uint32_t group_points = kSplatTile * rounds;
         for (uint32_t group = blockIdx.x; (unsigned long long)group * group_points < points; group += gridDim.x) {
             const uint32_t r0 = a.tile_first_rank[group * rounds];
-#if GPS_SPLAT_TILE_PREFETCH
-            if (binned && threadIdx.x < 32u) {
-                // the splat-buffer tile under this block's next group (the tile of its first
-                // survivor's pixel mean, where most of its samples land) heads for L2 now
-                const uint32_t ng = group + gridDim.x;
-                if ((unsigned long long)ng * group_points < points) {
-                    const uint32_t g = __ldg(&gids[a.tile_first_rank[ng * rounds]]);
-                    const float2 pm = __ldg(reinterpret_cast<const float2*>(a.records + min(g, a.n - 1u)));
-                    const uint32_t tx = (uint32_t)((int)pm.x >> kTileBits), ty = (uint32_t)((int)pm.y >> kTileBits);
-                    if (tx < a.tiles_x && ty < a.tiles_y) {
-                        const char* base = reinterpret_cast<const char*>(a.buffer + (uint64_t)(ty * a.tiles_x + tx) * a.tile_words);
-                        for (uint32_t line = threadIdx.x; line < a.tile_lines; line += 32u) prefetch_l2(base + (uint64_t)line * 128u);
-                    }
-                }
-            }
-#endif
 #pragma unroll
             for (uint32_t q = 0; q < rounds; ++q)
                 s_start[q * kSplatTile + threadIdx.x] = start_of(r0, q * kSplatTile + threadIdx.x);

@@ -151,8 +151,6 @@ struct SplatArgs {
     unsigned long long* clear_b;
     uint32_t clear_b_words;
     uint32_t* mask_iter;             // advanced after a pass with points (null: not here)
-    // splat-buffer tiles: per row and column, entries and 128-byte lines per tile
-    uint32_t tiles_x, tiles_y, tile_words, tile_lines;
 };
 
 // Screen bins: the splat walks a pass's survivors grouped by the 64x64 splat-buffer tile (or

@@ -416,31 +416,59 @@ uint32_t gaussians_per_block(uint64_t n) {
 }
 
 SceneBounds compute_scene_bounds(const CpuGaussian* g, uint64_t n) {
-    SceneBounds b;
-    const float lo = -FLT_MAX, hi = FLT_MAX;
-    b.max_pos = make_v3(lo, lo, lo);
-    b.min_pos = make_v3(hi, hi, hi);
-    b.max_scale = make_v3(lo, lo, lo);
-    b.min_scale = make_v3(hi, hi, hi);
-    for (int i = 0; i < 15; ++i) {
-        b.max_sh[i] = make_v3(lo, lo, lo);
-        b.min_sh[i] = make_v3(hi, hi, hi);
-    }
+    auto fresh = []() {
+        SceneBounds b;
+        const float lo = -FLT_MAX, hi = FLT_MAX;
+        b.max_pos = make_v3(lo, lo, lo);
+        b.min_pos = make_v3(hi, hi, hi);
+        b.max_scale = make_v3(lo, lo, lo);
+        b.min_scale = make_v3(hi, hi, hi);
+        for (int i = 0; i < 15; ++i) {
+            b.max_sh[i] = make_v3(lo, lo, lo);
+            b.min_sh[i] = make_v3(hi, hi, hi);
+        }
+        return b;
+    };
+    // gmin / gmax keep the running value unless the new one is strictly smaller / larger (and a
+    // NaN never is), so a fold keeps the earliest extreme value.  Folding contiguous ranges in
+    // parallel and then the ranges' results left to right keeps the same one: the result is the
+    // sequential fold's, bit for bit (signed zeros included).
     auto vmax = [](vec3 a, vec3 c) { return make_v3(gmax(a.x, c.x), gmax(a.y, c.y), gmax(a.z, c.z)); };
     auto vmin = [](vec3 a, vec3 c) { return make_v3(gmin(a.x, c.x), gmin(a.y, c.y), gmin(a.z, c.z)); };
-    for (uint64_t i = 0; i < n; ++i) {
-        vec3 m = make_v3(g[i].mean[0], g[i].mean[1], g[i].mean[2]);
-        b.max_pos = vmax(b.max_pos, m);
-        b.min_pos = vmin(b.min_pos, m);
-        vec3 ls = make_v3(std::log(g[i].scale[0]), std::log(g[i].scale[1]), std::log(g[i].scale[2]));
-        b.max_scale = vmax(b.max_scale, ls);
-        b.min_scale = vmin(b.min_scale, ls);
+    auto merge = [&](SceneBounds& b, const SceneBounds& c) {
+        b.max_pos = vmax(b.max_pos, c.max_pos);
+        b.min_pos = vmin(b.min_pos, c.min_pos);
+        b.max_scale = vmax(b.max_scale, c.max_scale);
+        b.min_scale = vmin(b.min_scale, c.min_scale);
         for (int j = 0; j < 15; ++j) {
-            vec3 s = make_v3(g[i].sh[3 * j + 3], g[i].sh[3 * j + 4], g[i].sh[3 * j + 5]);
-            b.max_sh[j] = vmax(b.max_sh[j], s);
-            b.min_sh[j] = vmin(b.min_sh[j], s);
+            b.max_sh[j] = vmax(b.max_sh[j], c.max_sh[j]);
+            b.min_sh[j] = vmin(b.min_sh[j], c.min_sh[j]);
         }
-    }
+    };
+    auto fold = [&](uint64_t lo_i, uint64_t hi_i, SceneBounds& b) {
+        for (uint64_t i = lo_i; i < hi_i; ++i) {
+            vec3 m = make_v3(g[i].mean[0], g[i].mean[1], g[i].mean[2]);
+            b.max_pos = vmax(b.max_pos, m);
+            b.min_pos = vmin(b.min_pos, m);
+            vec3 ls = make_v3(std::log(g[i].scale[0]), std::log(g[i].scale[1]), std::log(g[i].scale[2]));
+            b.max_scale = vmax(b.max_scale, ls);
+            b.min_scale = vmin(b.min_scale, ls);
+            for (int j = 0; j < 15; ++j) {
+                vec3 s = make_v3(g[i].sh[3 * j + 3], g[i].sh[3 * j + 4], g[i].sh[3 * j + 5]);
+                b.max_sh[j] = vmax(b.max_sh[j], s);
+                b.min_sh[j] = vmin(b.min_sh[j], s);
+            }
+        }
+    };
+    const uint64_t ranges = n < 65536 ? 1 : std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
+    std::vector<SceneBounds> part(ranges, fresh());
+    const uint64_t per = (n + ranges - 1) / ranges;
+    std::vector<std::thread> ts;
+    for (uint64_t r = 0; r < ranges; ++r)
+        ts.emplace_back([&, r]() { fold(std::min(n, r * per), std::min(n, (r + 1) * per), part[r]); });
+    for (auto& t : ts) t.join();
+    SceneBounds b = fresh();
+    for (const SceneBounds& p : part) merge(b, p);
     const float margin = 0.001f;
     b.max_pos = make_v3(b.max_pos.x + margin, b.max_pos.y + margin, b.max_pos.z + margin);
     b.min_pos = make_v3(b.min_pos.x - margin, b.min_pos.y - margin, b.min_pos.z - margin);

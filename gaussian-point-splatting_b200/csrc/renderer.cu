@@ -517,10 +517,6 @@ void render_pass(gps_renderer* r, const FrameConst& fc, int frame, bool first, c
     sp.clear_b = binned ? r->bins.get() : nullptr;
     sp.clear_b_words = binned ? nbins : 0u;
     sp.mask_iter = r->mask_iter.get();
-    sp.tiles_x = (uint32_t)((fc.up_width + kTileSize - 1) >> kTileBits);
-    sp.tiles_y = (uint32_t)((fc.up_height + kTileSize - 1) >> kTileBits);
-    sp.tile_words = (uint32_t)(kTileSize * kTileSize) * (uint32_t)fc.num_passes;
-    sp.tile_lines = sp.tile_words * 8u / 128u;
     launch_splat(sp, r->splat_grid, 256, st);
     count_launch(r, kStSplat);
 }
