@@ -1160,15 +1160,21 @@ __global__ void __launch_bounds__(256) resolve_morton_kernel(ResolveArgs a, int 
 // word after each pixel's samples keeps the threads of a warp, which read samples a whole
 // pixel run apart, on different banks.  Used when SS*SS*spp is a power of two >= 2.
 constexpr int kResolveStageBytes = 48 * 1024;
+#ifndef GPS_RESOLVE_REVERSED
+#define GPS_RESOLVE_REVERSED 1
+#endif
 #ifndef GPS_RESOLVE_PIXELS
-#define GPS_RESOLVE_PIXELS 128
+#define GPS_RESOLVE_PIXELS 64
 #endif
 
 template <bool kDepthOnly>
 __global__ void __launch_bounds__(256) resolve_staged_kernel(ResolveArgs a, int ss_log2, int run_log2) {
     extern __shared__ uint64_t stage[];
     const uint32_t run = 1u << run_log2;                            // entries per pixel
-    const uint32_t g0 = blockIdx.x * blockDim.x;
+    // blocks take the buffer from its end: the splat walks screen bins (buffer tiles) in
+    // ascending order, so the tiles it touched last are the ones still in L2
+    const uint32_t bid = GPS_RESOLVE_REVERSED ? gridDim.x - 1u - blockIdx.x : blockIdx.x;
+    const uint32_t g0 = bid * blockDim.x;
     const uint64_t first = (uint64_t)g0 * run;
     uint64_t last = first + (uint64_t)blockDim.x * run;
     if (last > a.entries) last = a.entries;
