@@ -343,7 +343,8 @@ __global__ void __launch_bounds__(256) preprocess_kernel(PreprocessArgs a, Scene
             tile_s += (uint32_t)__popc(m);
             tile_p += __reduce_add_sync(0xffffffffu, pts);
         }
-        if (a.bins && m) {  // one atomic per distinct bin among the warp's survivors
+        if (a.bins && m) {  // one atomic per distinct bin cursor among the warp's survivors
+            bin += (c & ((1u << a.bin_sub_log2) - 1u)) * a.bin_count;  // this chunk's cursor of each bin
             unsigned todo = m;
             while (todo) {
                 const uint32_t key = __shfl_sync(0xffffffffu, bin, __ffs(todo) - 1);
@@ -479,11 +480,19 @@ __global__ void __launch_bounds__(kScanThreads) scan_reduce_kernel(ScanArgs a) {
 // each thread scans 4 consecutive words and a block scan plus a running carry joins them.
 constexpr int kTileScanThreads = 1024;
 constexpr int kTileScanPer = 4;
+static_assert(kBinSubs <= (uint32_t)kTileScanPer && (kBinSubs & (kBinSubs - 1u)) == 0u,
+              "a scan thread's words must hold whole bins");
 
 // One block: exclusive prefix of `count` packed (survivors << 32 | points) words in place,
 // through shared memory in coalesced rounds; returns the totals.
+// Scans words_g in the order of its logical index L; with sub_log2 > 0, word L is stored at
+// (L mod 2^sub_log2) * stride + L / 2^sub_log2 (the bin cursors' layout).
 __device__ __forceinline__ void scan_words_inplace(unsigned long long* words_g, uint32_t count, uint32_t& total_s,
-                                                   uint32_t& total_p, uint32_t* max_s = nullptr) {
+                                                   uint32_t& total_p, uint32_t* max_s = nullptr,
+                                                   uint32_t sub_log2 = 0, uint32_t stride = 0) {
+    auto at = [&](uint32_t L) -> uint32_t {
+        return sub_log2 ? (L & ((1u << sub_log2) - 1u)) * stride + (L >> sub_log2) : L;
+    };
     __shared__ unsigned long long words[kTileScanThreads * kTileScanPer];
     __shared__ uint32_t s_max;
     constexpr uint32_t kRound = kTileScanThreads * kTileScanPer;
@@ -491,15 +500,19 @@ __device__ __forceinline__ void scan_words_inplace(unsigned long long* words_g, 
     if (threadIdx.x == 0) s_max = 0;
     for (uint32_t r0 = 0; r0 < count; r0 += kRound) {
         for (uint32_t i = threadIdx.x; i < kRound; i += kTileScanThreads)
-            words[i] = r0 + i < count ? words_g[r0 + i] : 0ull;
+            words[i] = r0 + i < count ? words_g[at(r0 + i)] : 0ull;
         __syncthreads();
-        uint32_t s = 0, p = 0;
+        uint32_t s = 0, p = 0, group = 0;
 #pragma unroll
         for (int k = 0; k < kTileScanPer; ++k) {
             const unsigned long long v = words[threadIdx.x * kTileScanPer + k];
             s += (uint32_t)(v >> 32);
             p += (uint32_t)v;
-            my_max = max(my_max, (uint32_t)(v >> 32));
+            group += (uint32_t)(v >> 32);
+            if ((((uint32_t)k + 1u) & ((1u << sub_log2) - 1u)) == 0u) {  // a whole bin's cursors
+                my_max = max(my_max, group);
+                group = 0;
+            }
         }
         uint32_t ex_s, ex_p, tot_s, tot_p;
         block_scan_pair<kTileScanThreads>(s, p, ex_s, ex_p, tot_s, tot_p);
@@ -513,14 +526,14 @@ __device__ __forceinline__ void scan_words_inplace(unsigned long long* words_g, 
             ex_p += (uint32_t)v;
         }
         __syncthreads();
-        for (uint32_t i = threadIdx.x; i < kRound && r0 + i < count; i += kTileScanThreads) words_g[r0 + i] = words[i];
+        for (uint32_t i = threadIdx.x; i < kRound && r0 + i < count; i += kTileScanThreads) words_g[at(r0 + i)] = words[i];
         carry_s += tot_s;
         carry_p += tot_p;
         __syncthreads();
     }
     total_s = carry_s;
     total_p = carry_p;
-    if (max_s) {  // the largest survivor count of one word
+    if (max_s) {  // the largest survivor count of one bin (2^sub_log2 consecutive words)
         my_max = __reduce_max_sync(0xffffffffu, my_max);
         if ((threadIdx.x & 31u) == 0u) atomicMax(&s_max, my_max);
         __syncthreads();
@@ -535,9 +548,9 @@ __global__ void __launch_bounds__(kTileScanThreads) scan_tiles_kernel(ScanArgs a
     uint32_t carry_s, carry_p;
     if (blockIdx.x == 1) {
         uint32_t most = 0;
-        scan_words_inplace(a.bins, a.nbins, carry_s, carry_p, &most);
-        // a bin crowded past bin_crowded survivors would serialise the downsweep on its cursor:
-        // the pass is then walked in Gaussian order
+        scan_words_inplace(a.bins, a.nbins, carry_s, carry_p, &most, (uint32_t)a.bin_sub_log2, a.bin_count);
+        // a bin crowded past bin_crowded survivors would serialise the downsweep on its
+        // cursors: the pass is then walked in Gaussian order
         if (threadIdx.x == 0) a.counters->crowded = most > a.bin_crowded ? 1u : 0u;
         return;
     }
@@ -640,7 +653,8 @@ __global__ void __launch_bounds__(kScanThreads) scan_write_fused_kernel(ScanArgs
                 a.surv_start[r] = pt;
                 if (binned) {
                     const float2 pm = __ldg(reinterpret_cast<const float2*>(a.records + g));
-                    const uint32_t bin = screen_bin(pm.x, pm.y, a.up_width, a.up_height, a.bin_shift, a.bins_x, a.bins_y);
+                    const uint32_t bin = screen_bin(pm.x, pm.y, a.up_width, a.up_height, a.bin_shift, a.bins_x, a.bins_y) +
+                                         ((g >> 5) & ((1u << a.bin_sub_log2) - 1u)) * a.bin_count;
                     const unsigned long long old = atomicAdd(a.bins + bin, (1ull << 32) | cnt[i]);
                     const uint32_t slot = (uint32_t)(old >> 32);
                     a.sorted_gid[slot] = g;

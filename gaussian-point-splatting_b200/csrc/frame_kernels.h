@@ -98,6 +98,8 @@ struct PreprocessArgs {
     int tile_shift;
     unsigned long long* bins;
     int bin_shift, bins_x, bins_y;
+    int bin_sub_log2;  // each screen bin has 2^bin_sub_log2 cursors (see kBinSubs)
+    uint32_t bin_count;  // bins_x * bins_y
 };
 
 struct ScanArgs {
@@ -123,6 +125,8 @@ struct ScanArgs {
     unsigned long long* bins;
     uint32_t nbins;
     int bin_shift, bins_x, bins_y, up_width, up_height;
+    int bin_sub_log2;            // cursors per screen bin, log2 (see kBinSubs)
+    uint32_t bin_count;          // bins_x * bins_y (nbins = bin_count << bin_sub_log2)
     const SplatRecord* records;
     uint32_t* sorted_gid;        // [n] survivors in bin order
     uint32_t* sorted_pstart;     //     their first points (reference point indices)
@@ -162,9 +166,19 @@ constexpr uint32_t kMaxBins = 16384;  // screen bins per pass (bins widen beyond
 #define GPS_BIN_CROWDED 131072
 #endif
 // Survivors of one bin past which binning costs more than it saves: each takes its place with
-// an atomic on the bin's cursor, and those serialise (about 1.7 ns each).  The environment
+// an atomic on one of the bin's cursors, and those serialise.  The environment
 // variable GPS_BIN_CROWDED overrides it when a renderer is created.
 constexpr uint32_t kBinCrowded = GPS_BIN_CROWDED;
+// Cursors per screen bin (at most; fewer where bins x cursors would pass kMaxBins): a survivor
+// takes its place on cursor (its 32-Gaussian chunk mod kBinSubs), so that the survivors of one
+// bin spread their atomics over that many addresses.  Cursor k of bin b is stored at word
+// k * bin_count + b, so that a bin's cursors sit in different cache lines (L2 slices), while the
+// order takes them as (b, k): a bin's cursors are consecutive and the walk still takes the bin
+// as a unit.
+#ifndef GPS_BIN_SUBS
+#define GPS_BIN_SUBS 4
+#endif
+constexpr uint32_t kBinSubs = GPS_BIN_SUBS;  // a power of two, at most 4 (the bin scan's words per thread)
 #ifndef GPS_SPLAT_BINNED
 #define GPS_SPLAT_BINNED 1
 #endif

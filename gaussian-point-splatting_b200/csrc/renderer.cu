@@ -444,11 +444,16 @@ void render_pass(gps_renderer* r, const FrameConst& fc, int frame, bool first, c
         ++bin_shift;
     const int bins_x = (fc.up_width + (1 << bin_shift) - 1) >> bin_shift;
     const int bins_y = (fc.up_height + (1 << bin_shift) - 1) >> bin_shift;
-    const uint32_t nbins = (uint32_t)(bins_x * bins_y);
+    int bin_sub_log2 = 0;  // cursors per bin, within kMaxBins words
+    while ((1u << (bin_sub_log2 + 1)) <= kBinSubs && ((uint64_t)bins_x * bins_y << (bin_sub_log2 + 1)) <= kMaxBins)
+        ++bin_sub_log2;
+    const uint32_t nbins = (uint32_t)(bins_x * bins_y) << bin_sub_log2;
     pa.tile_totals = r->tile_state.get();
     pa.tile_shift = scan_tile_shift(r->n);
     pa.bins = binned ? r->bins.get() : nullptr;
     pa.bin_shift = bin_shift;
+    pa.bin_sub_log2 = bin_sub_log2;
+    pa.bin_count = (uint32_t)(bins_x * bins_y);
     pa.bins_x = bins_x;
     pa.bins_y = bins_y;
     if (r->scene->format == GPS_SCENE_FP32) {
@@ -488,6 +493,8 @@ void render_pass(gps_renderer* r, const FrameConst& fc, int frame, bool first, c
     sa.bin_crowded = r->bin_crowded;
     sa.nbins = nbins;
     sa.bin_shift = bin_shift;
+    sa.bin_sub_log2 = bin_sub_log2;
+    sa.bin_count = (uint32_t)(bins_x * bins_y);
     sa.bins_x = bins_x;
     sa.bins_y = bins_y;
     sa.up_width = fc.up_width;
