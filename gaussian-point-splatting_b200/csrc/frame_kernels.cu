@@ -1016,10 +1016,10 @@ __global__ void __launch_bounds__(kSplatTile, kSplatRounds > 1 ? (K >= 8 ? 2 : G
         a.clear_b[i] = 0ull;
     if (a.mask_iter && points > 0u && blockIdx.x == 0 && threadIdx.x == 0) *a.mask_iter += 1u;
     // splats walk position q0 + threadIdx.x of a tile whose survivor starts are in `starts`
-    auto splat_tile_point = [&](uint32_t q0, uint32_t r0, const uint32_t* starts, int window) {
+    auto splat_tile_point = [&](uint32_t q0, uint32_t r0, const uint32_t* starts, int window, int lo0, int hi0) {
         const uint32_t q = q0 + threadIdx.x;
         if (q < points && starts[0] <= q) {
-            int lo = 0, hi = window - 1;  // largest k with starts[k] <= q
+            int lo = lo0, hi = hi0;  // largest k with starts[k] <= q
             while (lo < hi) {
                 int mid = (lo + hi + 1) >> 1;
                 if (starts[mid] <= q) lo = mid;
@@ -1060,8 +1060,17 @@ __global__ void __launch_bounds__(kSplatTile, kSplatRounds > 1 ? (K >= 8 ? 2 : G
             for (uint32_t q = 0; q < rounds; ++q)
                 s_start[q * kSplatTile + threadIdx.x] = start_of(r0, q * kSplatTile + threadIdx.x);
             __syncthreads();
-            for (uint32_t q = 0; q < rounds; ++q)
-                splat_tile_point(group * group_points + q * kSplatTile, r0, s_start, (int)group_points);
+            for (uint32_t q = 0; q < rounds; ++q) {
+                // the tile's points belong to the owners of its first point and of the next
+                // tile's first point, and to those between: the owner search starts from that
+                // range (splat 1.562 -> 1.545 ms/frame on the 16M orbit)
+                const uint32_t t = group * rounds + q;
+                int hi0 = (int)group_points - 1;
+                const int lo0 = min((int)(__ldg(&a.tile_first_rank[t]) - r0), hi0);
+                if ((unsigned long long)(t + 1) * kSplatTile < points)
+                    hi0 = max(lo0, min((int)(__ldg(&a.tile_first_rank[t + 1]) - r0), hi0));
+                splat_tile_point(group * group_points + q * kSplatTile, r0, s_start, (int)group_points, lo0, hi0);
+            }
             __syncthreads();
         }
     };
