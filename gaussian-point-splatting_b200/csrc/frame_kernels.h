@@ -182,6 +182,13 @@ constexpr uint32_t kBinSubs = GPS_BIN_SUBS;  // a power of two, at most 4 (the b
 #ifndef GPS_SPLAT_BINNED
 #define GPS_SPLAT_BINNED 1
 #endif
+// Views whose splat buffer is smaller than this are walked in Gaussian order: their buffer
+// stays in L2 whatever the order, and their few bins (60 at 640x360) would put every cursor
+// atomic of the pass on a handful of cache lines.
+#ifndef GPS_BIN_MIN_BUFFER_MB
+#define GPS_BIN_MIN_BUFFER_MB 64
+#endif
+constexpr uint64_t kBinMinBufferBytes = (uint64_t)GPS_BIN_MIN_BUFFER_MB << 20;
 #ifndef GPS_BIN_SHIFT
 #define GPS_BIN_SHIFT 6  // log2 of the bin width in pixels: one 64x64 splat-buffer tile
 #endif

@@ -407,6 +407,11 @@ void count_launch(gps_renderer* r, int stage, uint64_t n = 1) {
     r->timer.launches[stage] += n;
 }
 
+// Whether the view's passes walk their survivors in screen-bin order (see kBinMinBufferBytes).
+bool screen_binned(const gps_renderer* r) {
+    return GPS_SPLAT_BINNED != 0 && r->entries * sizeof(uint64_t) >= kBinMinBufferBytes;
+}
+
 void render_pass(gps_renderer* r, const FrameConst& fc, int frame, bool first, cudaStream_t st) {
     const int frame_seed = 4 * frame + (first ? 0 : 2);
     BlockView blocks = block_view(r);
@@ -437,7 +442,7 @@ void render_pass(gps_renderer* r, const FrameConst& fc, int frame, bool first, c
     pa.buffer = r->buffer.get();
     pa.loaded = r->loaded.get();
     // screen bins for this view: one 64x64 splat-buffer tile each, wider for very large views
-    const bool binned = GPS_SPLAT_BINNED != 0;
+    const bool binned = screen_binned(r);
     int bin_shift = GPS_BIN_SHIFT;
     while ((uint64_t)((fc.up_width + (1 << bin_shift) - 1) >> bin_shift) *
                (uint64_t)((fc.up_height + (1 << bin_shift) - 1) >> bin_shift) > kMaxBins)
@@ -1030,7 +1035,7 @@ gps_status gps_renderer_stats(gps_renderer* r, gps_stats* out) {
     out->kernel_launches = (int32_t)r->frame_launches;
     out->gaussians_read_one = (int32_t)c[0].loaded;
     out->gaussians_read_two = (int32_t)c[1].loaded;
-    const bool binned = GPS_SPLAT_BINNED != 0;
+    const bool binned = screen_binned(r);
     out->screen_order_one = (binned && c[0].points && !c[0].truncated && !c[0].crowded) ? 1 : 0;
     out->screen_order_two = (binned && c[1].points && !c[1].truncated && !c[1].crowded) ? 1 : 0;
     if (out->device_timeouts) return fail(GPS_ERR_DEVICE_TIMEOUT, "a device-side look-back wait gave up");

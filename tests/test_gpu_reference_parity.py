@@ -96,7 +96,8 @@ def _bits(words, n):
 
 
 # the walk order each case must exercise in every frame's passes (1 = screen-bin order)
-SCREEN_ORDER = {"c2_town2m_1080p": 1, "c2_town2m_crowded": 0}
+# (a 640x360 view's buffer stays in L2 and is walked in Gaussian order)
+SCREEN_ORDER = {"c2_town2m_1080p": 1, "c2_town2m_crowded": 0, "c1_cube1m": 0}
 
 
 @pytest.mark.parametrize("case", sorted(CASES))
