@@ -621,9 +621,17 @@ __device__ __forceinline__ void own_tiles(uint32_t* __restrict__ tile_first_rank
 
 template <int kScanRounds>
 __global__ void __launch_bounds__(kScanThreads) scan_write_fused_kernel(ScanArgs a) {
+    const uint32_t tile = blockIdx.x;
+    // a tile without survivors (its exclusive survivor prefix equals the next tile's) has
+    // nothing to write: culled regions of the scene cost two loads, not a pass over their masks
+    // (256M town: scan 0.586 -> 0.548 ms/frame)
+    {
+        const uint32_t s0 = (uint32_t)(a.tile_state[tile] >> 32);
+        const uint32_t s1 = tile + 1u < gridDim.x ? (uint32_t)(a.tile_state[tile + 1u] >> 32) : a.counters->survivors;
+        if (s0 == s1) return;
+    }
     const uint32_t* mask = a.mask;
     if (a.mask_iter) mask = (*a.mask_iter & 1u) ? a.mask_pair[1] : a.mask_pair[0];
-    const uint32_t tile = blockIdx.x;
     const uint32_t base = tile * (kScanThreads * kScanItems * kScanRounds) + threadIdx.x * (kScanItems * kScanRounds);
     uint32_t surv = 0, pts = 0;
 #pragma unroll
