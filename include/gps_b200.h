@@ -120,8 +120,12 @@ typedef struct gps_stats {
                                                        pass 2's previous-mask test) */
     int32_t screen_order_one, screen_order_two;     /* 1 if the pass's splat walked its survivors
                                                        in screen-bin order, 0 in Gaussian order
-                                                       (budget-truncated pass, or a bin crowded
-                                                       past 131,072 survivors) */
+                                                       (a splat buffer under 64 MB, a
+                                                       budget-truncated pass, or a bin crowded
+                                                       past 131,072 survivors; the environment
+                                                       variable GPS_BIN_CROWDED, read when a
+                                                       renderer is created, overrides that
+                                                       count).  The order changes no output. */
 } gps_stats;
 
 typedef struct gps_scene gps_scene;
