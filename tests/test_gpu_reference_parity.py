@@ -81,6 +81,13 @@ CASES = {
     "c2_town2m_1080p": ("town2m", lambda: synth.town(2_000_000, seed=5), dict(width=1920, height=1080,
                         supersampling_factor=2, samples_per_pixel=4, accumulation_mode=gpsplat.GPS_ACCUM_TAA),
                         synth.orbit(3, 30.0, 10.0), "fp32", gpsplat.GPS_SCENE_FP32),
+    # 4K: 8160 screen bins, so two cursors per bin (not four); a 531 MB splat buffer
+    "town2m_4k_ss2_spp2": ("town2m", lambda: synth.town(2_000_000, seed=5), dict(width=3840, height=2160,
+                           supersampling_factor=2, samples_per_pixel=2, accumulation_mode=gpsplat.GPS_ACCUM_TAA),
+                           synth.orbit(2, 30.0, 10.0), "fp32", gpsplat.GPS_SCENE_FP32),
+    # supersampling 3: K = 9 points per thread (the general splat path) and the row-major resolve
+    "town_ss3": ("town60k", lambda: synth.town(60000, seed=5), dict(width=213, height=120, supersampling_factor=3,
+                 samples_per_pixel=2), synth.orbit(3, 30.0, 10.0), "fp32", gpsplat.GPS_SCENE_FP32),
     # the same with the Gaussian-order walk that a pass falls back to when a screen bin is crowded
     "c2_town2m_crowded": ("town2m", lambda: synth.town(2_000_000, seed=5), dict(width=1920, height=1080,
                           supersampling_factor=2, samples_per_pixel=4, accumulation_mode=gpsplat.GPS_ACCUM_TAA),
@@ -97,7 +104,7 @@ def _bits(words, n):
 
 # the walk order each case must exercise in every frame's passes (1 = screen-bin order)
 # (a 640x360 view's buffer stays in L2 and is walked in Gaussian order)
-SCREEN_ORDER = {"c2_town2m_1080p": 1, "c2_town2m_crowded": 0, "c1_cube1m": 0}
+SCREEN_ORDER = {"c2_town2m_1080p": 1, "c2_town2m_crowded": 0, "c1_cube1m": 0, "town2m_4k_ss2_spp2": 1}
 
 
 @pytest.mark.parametrize("case", sorted(CASES))
