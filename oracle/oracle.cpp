@@ -1,7 +1,7 @@
 // CPU oracle of the Gaussian point-splatting frame path — TEST INFRASTRUCTURE ONLY.
 //
 // A plain C++ restatement of the reference's algorithm (PeterZs/gaussian-point-splatting),
-// used by tests/ and by bench.py's CPU-baseline leg as the checker; nothing in the library
+// used by tests/ and by bench.py's CPU-baseline leg to check the CUDA path; nothing in the library
 // links or calls it.  It follows, step by step:
 //   frame driver        src/core/rendering/passes/gaussian_point_splatting.cu:599-737
 //   preprocess          gaussian_point_splatting.cu:17-65, 147-307
@@ -34,7 +34,7 @@
 
 #include "../include/gps_b200.h"
 
-// The estimator's arithmetic type: float for the FP32 oracle (the checker of the CUDA path),
+// The estimator's arithmetic type: float for the FP32 oracle (what the CUDA path is checked against),
 // double for the FP64 build (ORACLE_FP64, liboracle64.so) used to state arithmetic error.  The
 // integer layer (seeds, PCG, Morton addressing, packing, scan) is the same in both; scene storage,
 // the depth chain and the culling blocks stay FP32 in both.

@@ -1,7 +1,7 @@
 """ctypes wrapper of the CPU oracle (oracle/oracle.cpp) — TEST INFRASTRUCTURE ONLY.
 
-The oracle is the checker: tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg
-use it; the library never does.  Build with `make -C oracle` (done by __graft_entry__.build()).
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg use it, to check the
+CUDA path against; the library never does.  Build with `make -C oracle` (done by __graft_entry__.build()).
 """
 from __future__ import annotations
 
