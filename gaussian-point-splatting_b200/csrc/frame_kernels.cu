@@ -915,6 +915,80 @@ __device__ __forceinline__ bool draw_sample(u32x2& seed, const SampleConst& c, i
     return inside & !(alpha < 1.0f / 255.0f);
 }
 
+#ifndef GPS_SPLAT_PAIRED
+#define GPS_SPLAT_PAIRED 1  // splat 1.547 -> 1.480 ms/frame (16M), 4.74 -> 4.44 (256M)
+#endif
+// The K samples of a pass drawn two at a time: the random words come off the seed in stream
+// order, and the floating-point steps two samples share (the opacity-corrected inverse dilog
+// polynomial, the Box-Muller products, the pixel position and its offset) run as sm_100 paired
+// FP32 instructions (FFMA2 / FMUL2 / FADD2), each lane rounded as the scalar instruction would.
+// The transcendental and per-lane steps stay scalar.  Same values as draw_sample, bit for bit.
+template <int K>
+__device__ __forceinline__ void draw_samples_paired(u32x2& seed, const SampleConst& c, int p, uint32_t* slot,
+                                                    bool* live) {
+    static_assert(K % 2 == 0, "samples are drawn in pairs");
+    const float2 one = make_float2(1.0f, 1.0f);
+    const float2 li2 = make_float2(c.li2_alpha, c.li2_alpha);
+    const float2 inva = make_float2(c.inv_alpha, c.inv_alpha);
+    const float2 c0 = make_float2(c.c0, c.c0), c1 = make_float2(c.c1, c.c1), c2 = make_float2(c.c2, c.c2);
+    const float2 pmx = make_float2(c.pixel_mean.x, c.pixel_mean.x), pmy = make_float2(c.pixel_mean.y, c.pixel_mean.y);
+#pragma unroll
+    for (int j = 0; j < K; j += 2) {
+        u32x2 s0 = pcg2d_step(seed);
+        u32x2 s1 = pcg2d_step(s0);
+        seed = s1;
+        const float2 rk = make_float2(kRecip2e32, kRecip2e32);
+        const float2 ux = __fmul2_rn(make_float2((float)s0.x, (float)s1.x), rk);
+        const float2 uy = __fmul2_rn(make_float2((float)s0.y, (float)s1.y), rk);
+        // inv_dilog((1 - u.x) * Li2(alpha)) (random.cuh:110-127, 132-141)
+        const float2 x = __fmul2_rn(__fadd2_rn(one, make_float2(-ux.x, -ux.y)), li2);
+        const float2 t = make_float2(fminf(x.x / kLi2Max, 1.0f), fminf(x.y / kLi2Max, 1.0f));
+        float2 y = make_float2(-1.27463503e+01f, -1.27463503e+01f);
+        y = __ffma2_rn(y, t, make_float2(5.88993459e+01f, 5.88993459e+01f));
+        y = __ffma2_rn(y, t, make_float2(-1.16025780e+02f, -1.16025780e+02f));
+        y = __ffma2_rn(y, t, make_float2(1.26945827e+02f, 1.26945827e+02f));
+        y = __ffma2_rn(y, t, make_float2(-8.43108826e+01f, -8.43108826e+01f));
+        y = __ffma2_rn(y, t, make_float2(3.48799862e+01f, 3.48799862e+01f));
+        y = __ffma2_rn(y, t, make_float2(-8.89606235e+00f, -8.89606235e+00f));
+        y = __ffma2_rn(y, t, make_float2(1.38640936e+00f, 1.38640936e+00f));
+        y = __ffma2_rn(y, t, make_float2(-7.80640876e-01f, -7.80640876e-01f));
+        y = __ffma2_rn(y, t, make_float2(1.64841888e+00f, 1.64841888e+00f));
+        y = __ffma2_rn(y, t, make_float2(-2.82836687e-05f, -2.82836687e-05f));
+        const float2 a2 = __fmul2_rn(inva, y);
+        float r[2], sn[2], cs[2];
+#pragma unroll
+        for (int l = 0; l < 2; ++l) {
+            const float a = gclamp(l ? a2.y : a2.x, 1.e-37f, 1.0f);
+            r[l] = __fsqrt_rn(fmaxf(-2.0f * __logf(a), 0.0f));
+            __sincosf(2.0f * kPiF * (l ? uy.y : uy.x), &sn[l], &cs[l]);
+        }
+        const float2 rr = make_float2(r[0], r[1]);
+        const float2 xyx = __fmul2_rn(rr, make_float2(cs[0], cs[1]));
+        const float2 xyy = __fmul2_rn(rr, make_float2(sn[0], sn[1]));
+        const float2 px = __ffma2_rn(c0, xyx, pmx);
+        const float2 py = __ffma2_rn(c2, xyy, __ffma2_rn(c1, xyx, pmy));
+        const float2 fx = make_float2(floorf(px.x), floorf(px.y)), fy = make_float2(floorf(py.x), floorf(py.y));
+        const float2 dx = __fadd2_rn(pmx, make_float2(-fx.x, -fx.y));
+        const float2 dy = __fadd2_rn(pmy, make_float2(-fy.x, -fy.y));
+#pragma unroll
+        for (int l = 0; l < 2; ++l) {
+            const int xi = (int)(l ? fx.y : fx.x);
+            const int yi = (int)(l ? fy.y : fy.x);
+            const vec2 delta = make_v2(l ? dx.y : dx.x, l ? dy.y : dy.x);
+            const bool inside = ((uint32_t)xi - (uint32_t)c.minx < c.span_x) & ((uint32_t)yi - (uint32_t)c.miny < c.span_y);
+            const float alpha = c.opacity * gaussian_value(c.conic, delta);
+#if GPS_SPLAT_MORTON_LUT
+            const uint32_t code = c.spread[xi & (kTileSize - 1)] | (c.spread[yi & (kTileSize - 1)] << 1);
+#else
+            const uint32_t code = morton_encode((uint32_t)(xi & (kTileSize - 1)), (uint32_t)(yi & (kTileSize - 1)));
+#endif
+            const uint32_t tile = (uint32_t)((yi >> kTileBits) * c.tiles_per_row + (xi >> kTileBits));
+            slot[j + l] = (tile * (uint32_t)(kTileSize * kTileSize) + code) * (uint32_t)c.passes + (uint32_t)p;
+            live[j + l] = inside & !(alpha < 1.0f / 255.0f);
+        }
+    }
+}
+
 template <int K>
 __device__ __forceinline__ void splat_point_unbiased_k(uint32_t point, const SplatRecord& rec, const FrameConst& fc,
                                                        int frame_seed, uint64_t* __restrict__ buffer,
@@ -949,8 +1023,17 @@ __device__ __forceinline__ void splat_point_unbiased_k(uint32_t point, const Spl
     bool la[K], lb[K];
     unsigned long long va[K], vb[K];
     auto draw = [&](int p, uint32_t* sl, bool* lv, unsigned long long* vv) {
+#if GPS_SPLAT_PAIRED
+        if constexpr (K % 2 == 0) {
+            draw_samples_paired<K>(seed, c, p, sl, lv);
+        } else {
+#pragma unroll
+            for (int j = 0; j < K; ++j) lv[j] = draw_sample(seed, c, p, sl[j]);
+        }
+#else
 #pragma unroll
         for (int j = 0; j < K; ++j) lv[j] = draw_sample(seed, c, p, sl[j]);
+#endif
 #pragma unroll
         for (int j = 0; j < K; ++j)
             vv[j] = lv[j] ? (GPS_SPLAT_PRETEST == 1 ? __ldca(buf + sl[j]) : __ldcg(buf + sl[j])) : 0ull;
