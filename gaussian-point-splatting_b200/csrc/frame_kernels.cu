@@ -916,13 +916,14 @@ __device__ __forceinline__ bool draw_sample(u32x2& seed, const SampleConst& c, i
 }
 
 #ifndef GPS_SPLAT_PAIRED
-#define GPS_SPLAT_PAIRED 1  // splat 1.547 -> 1.480 ms/frame (16M), 4.74 -> 4.44 (256M)
+#define GPS_SPLAT_PAIRED 1  // splat 1.547 -> 1.461 ms/frame (16M)
 #endif
 // The K samples of a pass drawn two at a time: the random words come off the seed in stream
 // order, and the floating-point steps two samples share (the opacity-corrected inverse dilog
-// polynomial, the Box-Muller products, the pixel position and its offset) run as sm_100 paired
-// FP32 instructions (FFMA2 / FMUL2 / FADD2), each lane rounded as the scalar instruction would.
-// The transcendental and per-lane steps stay scalar.  Same values as draw_sample, bit for bit.
+// polynomial, the Box-Muller products, the pixel position and its offset, the Gaussian weight)
+// run as sm_100 paired FP32 instructions (FFMA2 / FMUL2 / FADD2), each lane rounded as the
+// scalar instruction would.  The transcendental and per-lane steps stay scalar.  Same values
+// as draw_sample, bit for bit.
 template <int K>
 __device__ __forceinline__ void draw_samples_paired(u32x2& seed, const SampleConst& c, int p, uint32_t* slot,
                                                     bool* live) {
@@ -956,11 +957,15 @@ __device__ __forceinline__ void draw_samples_paired(u32x2& seed, const SampleCon
         y = __ffma2_rn(y, t, make_float2(-2.82836687e-05f, -2.82836687e-05f));
         const float2 a2 = __fmul2_rn(inva, y);
         float r[2], sn[2], cs[2];
+        // -2 log(a) and the angle 2 pi u: one product each, paired (scaling by -2 is exact, so
+        // the pair equals the scalar (lg2(a) ln2) (-2) however the scalar form groups it)
+        const float2 lg = __fmul2_rn(make_float2(-2.0f, -2.0f), make_float2(__logf(gclamp(a2.x, 1.e-37f, 1.0f)),
+                                                                             __logf(gclamp(a2.y, 1.e-37f, 1.0f))));
+        const float2 th = __fmul2_rn(make_float2(2.0f * kPiF, 2.0f * kPiF), uy);
 #pragma unroll
         for (int l = 0; l < 2; ++l) {
-            const float a = gclamp(l ? a2.y : a2.x, 1.e-37f, 1.0f);
-            r[l] = __fsqrt_rn(fmaxf(-2.0f * __logf(a), 0.0f));
-            __sincosf(2.0f * kPiF * (l ? uy.y : uy.x), &sn[l], &cs[l]);
+            r[l] = __fsqrt_rn(fmaxf(l ? lg.y : lg.x, 0.0f));
+            __sincosf(l ? th.y : th.x, &sn[l], &cs[l]);
         }
         const float2 rr = make_float2(r[0], r[1]);
         const float2 xyx = __fmul2_rn(rr, make_float2(cs[0], cs[1]));
@@ -970,13 +975,23 @@ __device__ __forceinline__ void draw_samples_paired(u32x2& seed, const SampleCon
         const float2 fx = make_float2(floorf(px.x), floorf(px.y)), fy = make_float2(floorf(py.x), floorf(py.y));
         const float2 dx = __fadd2_rn(pmx, make_float2(-fx.x, -fx.y));
         const float2 dy = __fadd2_rn(pmy, make_float2(-fy.x, -fy.y));
+        // gaussian_value (linalg.cuh:309-317) on both samples.  Its sums of two products are fused
+        // as the compiler contracts them, the left product into the FMA: x*x-part first
+        // (fma(cx dx, dx, (cz dy) dy)), then fma(-0.5, quad, -((cy dx) dy)).  The tests pin this:
+        // fusing the right-hand products instead changed one entry of the 4K parity case.
+        const float2 cx = make_float2(c.conic.x, c.conic.x), cyv = make_float2(c.conic.y, c.conic.y),
+                     cz = make_float2(c.conic.z, c.conic.z);
+        const float2 quad = __ffma2_rn(__fmul2_rn(cx, dx), dx, __fmul2_rn(__fmul2_rn(cz, dy), dy));
+        const float2 hh = __fmul2_rn(__fmul2_rn(cyv, dx), dy);
+        const float2 sig = __ffma2_rn(make_float2(-0.5f, -0.5f), quad, make_float2(-hh.x, -hh.y));
+        const float2 gv = make_float2(sig.x > 0.f ? 0.0f : __expf(sig.x), sig.y > 0.f ? 0.0f : __expf(sig.y));
+        const float2 al = __fmul2_rn(make_float2(c.opacity, c.opacity), gv);
 #pragma unroll
         for (int l = 0; l < 2; ++l) {
             const int xi = (int)(l ? fx.y : fx.x);
             const int yi = (int)(l ? fy.y : fy.x);
-            const vec2 delta = make_v2(l ? dx.y : dx.x, l ? dy.y : dy.x);
             const bool inside = ((uint32_t)xi - (uint32_t)c.minx < c.span_x) & ((uint32_t)yi - (uint32_t)c.miny < c.span_y);
-            const float alpha = c.opacity * gaussian_value(c.conic, delta);
+            const float alpha = l ? al.y : al.x;
 #if GPS_SPLAT_MORTON_LUT
             const uint32_t code = c.spread[xi & (kTileSize - 1)] | (c.spread[yi & (kTileSize - 1)] << 1);
 #else
