@@ -608,7 +608,7 @@ __global__ void __launch_bounds__(kScanThreads) scan_write_kernel(ScanArgs a) {
 
 // The render path's downsweep: as scan_write_kernel, and then for every survivor the splat's
 // work order.  Screen-binned (bins set, pass not truncated): the survivor takes its slot and
-// first walk position from its bin's cursor with one 64-bit atomic, so that slot and position
+// first walk position from one of its bin's cursors with one 64-bit atomic, so that slot and position
 // stay consistent and positions increase with the slot; otherwise the Gaussian order itself,
 // with the points past P dropped as the reference drops them.  Either way the survivor then
 // records itself as the owner of every 256-point splat tile that starts inside its points.
