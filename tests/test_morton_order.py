@@ -64,6 +64,15 @@ def test_host_order_matches_oracle(name):
     assert np.array_equal(gpsplat.morton_order(g, on_device=False), oracle.morton_order(g))
 
 
+def test_host_order_with_nan_means_matches_oracle():
+    """A NaN coordinate never wins the bounds' comparisons and its key bits are 0 (the 21 low
+    bits of the conversion of NaN), as in the reference's host code."""
+    g = synth.activate(_shuffled(synth.cube(3000, seed=12), 8))
+    g[5, 0] = np.nan
+    g[100, 1:3] = np.nan
+    assert np.array_equal(gpsplat.morton_order(g, on_device=False), oracle.morton_order(g))
+
+
 def test_empty_scene_order():
     g = np.zeros((0, 59), np.float32)
     assert gpsplat.morton_order(g, on_device=False).size == 0
